@@ -1,0 +1,178 @@
+/*
+ * symprop.h — C ABI of the B200-native SymProp S3TTMc / Tucker path.
+ *
+ * Every entry point takes plain pointers and sizes and returns an int status
+ * (SYMPROP_OK == 0).  Host-pointer entry points copy inputs to the GPU and
+ * results back; *_device entry points take device pointers and a CUDA
+ * stream (cudaStream_t passed as void*, NULL = legacy default stream).
+ *
+ * The reference interface each entry point replaces is cited as
+ * <file>:<line> of the reference SymProp sources.
+ *
+ * Conventions carried over from the reference:
+ *   - index tuples are 1-based, sorted ascending inside each tuple
+ *     (src/utils/loader.cpp:29-31); ids must lie in [1, dim];
+ *   - U is row-major dim x R; Y is row-major dim x ldy, fully overwritten;
+ *   - packed Y has ldy = C(R+N-2, N-1) columns in lexicographic order of
+ *     sorted column indices (include/detail/dense/symtensor.hpp:58-62,
+ *     129-142); unpacked Y has ldy = R^(N-1) (src/sparse/spsymtensor.cpp:34-35).
+ */
+#ifndef SYMPROP_B200_H
+#define SYMPROP_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------- status */
+enum {
+  SYMPROP_OK = 0,
+  SYMPROP_ERR_INVALID = 1,   /* bad argument (null, out-of-range id, unsorted tuple, R = 0) */
+  SYMPROP_ERR_ORDER = 2,     /* unsupported order (the reference dispatcher throws
+                                std::out_of_range, include/utils/dispatcher.hpp:48-54) */
+  SYMPROP_ERR_OOM = 3,       /* device or pinned-host allocation failed */
+  SYMPROP_ERR_CUDA = 4,      /* a CUDA runtime call failed */
+  SYMPROP_ERR_NOCONV = 5,    /* an iterative FP64 solve did not converge
+                                (reference prints "... failed to converge",
+                                src/dense/matrixops.cpp:31-33,69-72,86-89) */
+  SYMPROP_ERR_TIMEOUT = 6,   /* a bounded device wait expired */
+  SYMPROP_ERR_SIZE = 7,      /* sizes beyond what this build supports */
+  SYMPROP_ERR_NODEVICE = 8   /* no CUDA device / the CUDA path is unavailable */
+};
+
+enum {
+  SYMPROP_FP64 = 0,          /* U, Y in double: the drop-in precision */
+  SYMPROP_FP32 = 1           /* U, Y in float, compensated FP32 accumulation */
+};
+
+enum { SYMPROP_HOOI = 0, SYMPROP_HOQRI = 1, SYMPROP_ALTHOOI = 2 };
+enum { SYMPROP_INIT_RND = 0, SYMPROP_INIT_HOEVD = 1, SYMPROP_INIT_HOSVD = 2,
+       SYMPROP_INIT_USER = 3 };
+enum { SYMPROP_PREC_FP64 = 0,   /* plain FP64 drop-in path */
+       SYMPROP_PREC_MIXED = 1   /* FP32 S3TTMc + 3xBF16 tcgen05 Gram + FP64 solves */ };
+
+/* Human-readable text for a status code and the last error of this thread. */
+const char *symprop_status_string(int status);
+const char *symprop_last_error(void);
+
+/* ------------------------------------------------------------- tensor */
+typedef struct symprop_tensor symprop_tensor;
+
+/* Builds the device-resident tensor: uploads the tuples, computes ||X|| and
+ * the row-segmented owner list used by S3TTMc (a device radix sort of the
+ * N owners of every nonzero by their remaining index).
+ * Replaces SpSymtensor::SpSymtensor (include/detail/sparse/spsymtensor.hpp:26-27,
+ * src/sparse/spsymtensor.cpp:16-28).  inds: nnz*order uint32, vals: nnz. */
+int symprop_tensor_create(uint32_t order, uint32_t dim, const uint32_t *inds,
+                          const double *vals, uint64_t nnz,
+                          symprop_tensor **out);
+int symprop_tensor_destroy(symprop_tensor *t);
+
+/* order/dim/size/norm accessors: include/detail/sparse/spsymtensor.hpp:29-34,43 */
+int symprop_tensor_order(const symprop_tensor *t, uint32_t *order);
+int symprop_tensor_dim(const symprop_tensor *t, uint32_t *dim);
+int symprop_tensor_nnz(const symprop_tensor *t, uint64_t *nnz);
+int symprop_tensor_norm(const symprop_tensor *t, double *norm);   /* SpSymtensor::norm, spsymtensor.cpp:112 */
+/* number of (row, leaf) owner records after merging repeated indices */
+int symprop_tensor_owner_count(const symprop_tensor *t, uint64_t *owners);
+
+/* ------------------------------------------------ CompressedDTree export */
+/* Builds, on the device (radix sort + unique + segmentation), the
+ * reference's CompressedDTree arrays for this tensor and keeps them until
+ * the tensor is destroyed.  Replaces DTree::banerjee_insert
+ * (src/dtree.cpp:56-80) + CompressedDTree::CompressedDTree
+ * (src/compressed_dtree.cpp:13-90) + init_dep_list (:92-131).
+ * depth = order - 1 levels; level l holds the sorted (l+1)-sub-multisets. */
+int symprop_tree_build(symprop_tensor *t);
+int symprop_tree_level_size(const symprop_tensor *t, uint32_t level, uint64_t *size);
+int symprop_tree_owner_count(const symprop_tensor *t, uint64_t *owners);
+/* Copies level_idx[level] (size), level_ptr[level] (size+1; for the last
+ * level the owner CSR) and dep_list[level] (size*(level+1); level >= 1) into
+ * host buffers.  Any pointer may be NULL. (compressed_dtree.hpp:52-57) */
+int symprop_tree_copy_level(const symprop_tensor *t, uint32_t level,
+                            uint32_t *level_idx, uint64_t *level_ptr,
+                            uint64_t *dep_list);
+/* Copies the owner list `nonzero` (compressed_dtree.hpp:59): remaining
+ * index (1-based) and value, in the reference's order. */
+int symprop_tree_copy_owners(const symprop_tensor *t, uint64_t *rem, double *val);
+
+/* ------------------------------------------------------------- S3TTMc */
+/* Y = X_(1) (U (x) ... (x) U), packed or unpacked, host buffers.
+ * Replaces SpSymtensor::S3TTMc (include/detail/sparse/spsymtensor.hpp:38-39,
+ * src/sparse/spsymtensor.cpp:30-110).  precision SYMPROP_FP64: U, Y are
+ * double*; SYMPROP_FP32: float*. */
+int symprop_s3ttmc(const symprop_tensor *t, const void *U, uint32_t R,
+                   int packed, void *Y, int precision);
+/* Same with device pointers on `stream`; Y is written asynchronously. */
+int symprop_s3ttmc_device(const symprop_tensor *t, const void *dU, uint32_t R,
+                          int packed, void *dY, int precision, void *stream);
+/* Number of kernel launches one symprop_s3ttmc_device call issues for
+ * (R, packed); lets callers count their launches. */
+int symprop_s3ttmc_launches(const symprop_tensor *t, uint32_t R, int packed,
+                            uint32_t *launches);
+
+/* ------------------------------------------------------ packed helpers */
+/* symtens_size (include/detail/dense/symtensor_base.hpp:28-30) */
+uint64_t symprop_symtens_size(uint32_t dim, uint32_t order);
+/* symtens_coeff (src/dense/symtensor.cpp:53-59): coeff[symtens_size] */
+int symprop_symtens_coeff(uint32_t dim, uint32_t order, double *coeff);
+/* unpack_symtens (src/dense/symtensor.cpp:40-45) on the device for
+ * `rows` rows: packed rows x C(dim+order-1,order) -> rows x dim^order. */
+int symprop_unpack_rows_device(const double *dpacked, uint64_t rows,
+                               uint32_t dim, uint32_t order, double *dfull,
+                               void *stream);
+
+/* ------------------------------------------------------------- Tucker */
+typedef struct {
+  uint32_t rank;      /* Config::rank     (include/detail/tucker.hpp:15) */
+  uint64_t max_iter;  /* Config::max_iter (tucker.hpp:16) */
+  double rel_tol;     /* Config::rel_tol  (tucker.hpp:17) */
+  double delta;       /* Config::delta    (tucker.hpp:18) */
+  uint64_t seed;      /* Config::seed     (tucker.hpp:19) */
+  int init;           /* Config::init: SYMPROP_INIT_* (tucker.hpp:20) */
+  int precision;      /* SYMPROP_PREC_FP64 (drop-in) or SYMPROP_PREC_MIXED */
+  int verbose;        /* print the reference's per-iteration lines to stdout */
+} symprop_config;
+
+typedef struct {
+  /* caller-owned outputs (may be NULL) */
+  double *core;        /* rank^order doubles: SymTuckerDecomp::_core (tucker.hpp:43) */
+  double *factor;      /* dim*rank doubles:  SymTuckerDecomp::_factor (tucker.hpp:44) */
+  double *error_trace; /* trace_cap doubles: error per iteration */
+  double *relres_trace;/* trace_cap doubles: relative residual per iteration */
+  uint64_t trace_cap;
+  const double *init_factor; /* dim*rank doubles when init == SYMPROP_INIT_USER */
+  /* filled in */
+  uint64_t iterations;
+  double error;        /* final sqrt(||X||^2-||C||^2)/||X|| (src/tucker.cpp:40-45) */
+  double core_norm;    /* ||C|| */
+  double time_ms;      /* device-timed duration of the whole solve */
+  double s3ttmc_ms;    /* device time spent in S3TTMc */
+  double dense_ms;     /* device time spent in the dense steps */
+} symprop_result;
+
+/* Runs HOOI / HOQRI / AltHOOI.  Replaces SpSymtensor::TuckerHOOI /
+ * TuckerHOQRI / TuckerAltHOOI (src/sparse/spsymtensor.cpp:201-252,
+ * 254-299, 301-337) including hosvd_init (:339-383) and the random
+ * SymTuckerDecomp factor (src/tucker.cpp:25-36). */
+int symprop_tucker(const symprop_tensor *t, const symprop_config *cfg, int alg,
+                   symprop_result *res);
+
+/* Writes the decomposition in the reference's text format
+ * (SymTuckerDecomp::print, src/tucker.cpp:47-61) to `path`
+ * ("stdout"/"stderr"/file; "" writes nothing). */
+int symprop_write_decomp(const char *path, const double *core,
+                         const double *factor, uint32_t dim, uint32_t rank,
+                         uint32_t order, int append);
+
+/* ------------------------------------------------------------- devices */
+int symprop_device_count(int *count);
+int symprop_set_device(int device);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SYMPROP_B200_H */

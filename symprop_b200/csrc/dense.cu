@@ -1,0 +1,691 @@
+// Dense steps of the Tucker loop on sm_100a (FP64 drop-in precision).
+//
+// Replaces the reference's CBLAS/LAPACKE wrappers
+// (src/dense/matrixops.cpp): gemmtn (:45-56), symgemm (:102-124) and
+// symsyrk (:126-146) become the tiled GEMM below; leftsvd (:18-43) and
+// syevd (:77-100) become a block-Krylov top-r eigensolver on the packed Gram
+// matrix with a one-CTA Jacobi for the projected problem; qr (:58-75)
+// becomes CholQR2 with a Householder QR fallback.
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "dense.cuh"
+
+namespace spb {
+namespace dense {
+
+namespace {
+
+inline unsigned cdiv(long long a, long long b) { return (unsigned)((a + b - 1) / b); }
+
+// ------------------------------------------------------------------- GEMM
+
+constexpr int BM = 64, BN = 64, BK = 16;
+
+template <typename T, bool TA, bool TB, bool KS>
+__global__ void __launch_bounds__(256) gemm_tile_kernel(int M, int N, int K, const T *__restrict__ A,
+                                                        int lda, const T *__restrict__ B, int ldb,
+                                                        const T *__restrict__ ks, T *out, int ldo,
+                                                        int kchunk, int sym_upper,
+                                                        size_t split_stride) {
+  const int tm = blockIdx.y, tn = blockIdx.x;
+  if (sym_upper && tm > tn) return;
+  const int bm = tm * BM, bn = tn * BN;
+  const int k0 = blockIdx.z * kchunk;
+  const int k1 = min(K, k0 + kchunk);
+  __shared__ T As[BK][BM + 1];
+  __shared__ T Bs[BK][BN + 1];
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  T acc[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j] = T(0);
+  for (int kk = k0; kk < k1; kk += BK) {
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      int idx = tid + e * 256;
+      int kq, im;
+      if (TA) { kq = idx / BM; im = idx % BM; } else { im = idx / BK; kq = idx % BK; }
+      int gi = bm + im, gk = kk + kq;
+      T v = T(0);
+      if (gi < M && gk < k1) {
+        v = TA ? A[(size_t)gk * lda + gi] : A[(size_t)gi * lda + gk];
+        if (KS) v *= ks[gk];
+      }
+      As[kq][im] = v;
+      int jn;
+      if (TB) { jn = idx / BK; kq = idx % BK; } else { kq = idx / BN; jn = idx % BN; }
+      int gj = bn + jn;
+      gk = kk + kq;
+      T w = T(0);
+      if (gj < N && gk < k1) w = TB ? B[(size_t)gj * ldb + gk] : B[(size_t)gk * ldb + gj];
+      Bs[kq][jn] = w;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kq = 0; kq < BK; ++kq) {
+      T a[4], b[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) a[i] = As[kq][ty * 4 + i];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) b[j] = Bs[kq][tx * 4 + j];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] += a[i] * b[j];
+    }
+    __syncthreads();
+  }
+  T *o = out + blockIdx.z * split_stride;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    int gi = bm + ty * 4 + i;
+    if (gi >= M) continue;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      int gj = bn + tx * 4 + j;
+      if (gj < N) o[(size_t)gi * ldo + gj] = acc[i][j];
+    }
+  }
+}
+
+// C = alpha * sum_z P[z] + beta * C, mirroring the lower triangle for sym_upper
+template <typename T>
+__global__ void gemm_finalize_kernel(int M, int N, const T *P, int splits, size_t stride, T alpha,
+                                     T beta, T *C, int ldc, int sym_upper) {
+  size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (size_t)M * N) return;
+  int i = (int)(idx / N), j = (int)(idx % N);
+  int si = i, sj = j;
+  if (sym_upper && (i / BM) > (j / BM)) { si = j; sj = i; }
+  T s = T(0);
+  for (int z = 0; z < splits; ++z) s += P[z * stride + (size_t)si * N + sj];
+  T prev = beta != T(0) ? C[(size_t)i * ldc + j] : T(0);
+  C[(size_t)i * ldc + j] = alpha * s + beta * prev;
+}
+
+// --------------------------------------------------------- reductions
+
+constexpr int kRedBlocks = 296;
+
+template <typename T>
+__global__ void wsq_partial_kernel(const T *X, const T *Y, const double *w, int rows, int cols,
+                                   double *part) {
+  double a = 0.0, b = 0.0;
+  size_t total = (size_t)rows * cols;
+  for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+       idx += (size_t)gridDim.x * blockDim.x) {
+    int q = (int)(idx % cols);
+    double x = (double)X[idx];
+    double d = x - (Y ? (double)Y[idx] : 0.0);
+    double ww = w ? w[q] : 1.0;
+    a += ww * d * d;
+    b += ww * x * x;
+  }
+  __shared__ double sa[256], sb[256];
+  sa[threadIdx.x] = a;
+  sb[threadIdx.x] = b;
+  __syncthreads();
+  for (int s = 128; s > 0; s >>= 1) {
+    if (threadIdx.x < s) {
+      sa[threadIdx.x] += sa[threadIdx.x + s];
+      sb[threadIdx.x] += sb[threadIdx.x + s];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    part[2 * blockIdx.x] = sa[0];
+    part[2 * blockIdx.x + 1] = sb[0];
+  }
+}
+
+__global__ void sum_pairs_kernel(const double *part, int n, double *out) {
+  __shared__ double sa[256], sb[256];
+  double a = 0, b = 0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    a += part[2 * i];
+    b += part[2 * i + 1];
+  }
+  sa[threadIdx.x] = a;
+  sb[threadIdx.x] = b;
+  __syncthreads();
+  for (int s = 128; s > 0; s >>= 1) {
+    if (threadIdx.x < s) {
+      sa[threadIdx.x] += sa[threadIdx.x + s];
+      sb[threadIdx.x] += sb[threadIdx.x + s];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    out[0] = sa[0];
+    out[1] = sb[0];
+  }
+}
+
+// ------------------------------------------------------------ Cholesky
+
+// G (c x c) -> Rinv (upper-triangular inverse of the Cholesky factor R,
+// G = R^T R).  status[0] = 1 when a pivot is not safely positive.
+__global__ void chol_inv_kernel(const double *G, int c, double *Rinv, int *status) {
+  extern __shared__ double sm[];
+  double *R = sm;          // c x c
+  double *Ri = sm + c * c; // c x c
+  const int tid = threadIdx.x, nt = blockDim.x;
+  for (int i = tid; i < c * c; i += nt) {
+    R[i] = G[i];
+    Ri[i] = 0.0;
+  }
+  __syncthreads();
+  __shared__ double maxd;
+  __shared__ int bad;
+  if (tid == 0) {
+    maxd = 0;
+    bad = 0;
+    for (int i = 0; i < c; ++i) maxd = fmax(maxd, fabs(R[i * c + i]));
+  }
+  __syncthreads();
+  // right-looking Cholesky on the upper triangle: R[k][k..] row k of R
+  for (int k = 0; k < c; ++k) {
+    if (tid == 0) {
+      double d = R[k * c + k];
+      if (!(d > 1e-13 * maxd) || !(maxd > 0)) {
+        bad = 1;
+        d = fmax(fabs(d), 1e-300);
+      }
+      R[k * c + k] = sqrt(d);
+    }
+    __syncthreads();
+    double rkk = R[k * c + k];
+    for (int j = k + 1 + tid; j < c; j += nt) R[k * c + j] /= rkk;
+    __syncthreads();
+    for (int idx = tid; idx < c * c; idx += nt) {
+      int i = idx / c, j = idx % c;
+      if (i > k && j >= i) R[i * c + j] -= R[k * c + i] * R[k * c + j];
+    }
+    __syncthreads();
+  }
+  // inverse of upper-triangular R: column by column back substitution
+  for (int j = tid; j < c; j += nt) {
+    for (int i = j; i >= 0; --i) {
+      double s = (i == j) ? 1.0 : 0.0;
+      for (int k = i + 1; k <= j; ++k) s -= R[i * c + k] * Ri[k * c + j];
+      Ri[i * c + j] = s / R[i * c + i];
+    }
+  }
+  __syncthreads();
+  for (int i = tid; i < c * c; i += nt) Rinv[i] = Ri[i];
+  if (tid == 0) status[0] = bad;
+}
+
+// ---------------------------------------------------- Householder (1 CTA)
+
+__device__ double block_sum(double v, double *red) {
+  const int tid = threadIdx.x;
+  red[tid] = v;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (tid < s) red[tid] += red[tid + s];
+    __syncthreads();
+  }
+  double r = red[0];
+  __syncthreads();
+  return r;
+}
+
+// A (rows x c) -> explicit Q as dgeqrf + dorgqr; v vectors kept in A,
+// Q built in Qout.  One CTA of 1024 threads; used for rank-deficient inputs.
+__global__ void __launch_bounds__(1024) householder_kernel(double *A, int rows, int c, double *tau,
+                                                           double *Q) {
+  __shared__ double red[1024];
+  const int tid = threadIdx.x, nt = blockDim.x;
+  for (int j = 0; j < c && j < rows; ++j) {
+    double s = 0;
+    for (int i = j + 1 + tid; i < rows; i += nt) s += A[(size_t)i * c + j] * A[(size_t)i * c + j];
+    double sigma = block_sum(s, red);
+    double alpha = A[(size_t)j * c + j];
+    double t = 0, beta = alpha;
+    if (sigma > 0) {
+      beta = -copysign(sqrt(alpha * alpha + sigma), alpha);
+      t = (beta - alpha) / beta;
+      double scal = 1.0 / (alpha - beta);
+      for (int i = j + 1 + tid; i < rows; i += nt) A[(size_t)i * c + j] *= scal;
+    }
+    __syncthreads();
+    if (tid == 0) {
+      tau[j] = t;
+      A[(size_t)j * c + j] = beta;
+    }
+    __syncthreads();
+    // apply H = I - t v v^T to columns j+1..c-1 (v[j] = 1)
+    for (int k = j + 1; k < c; ++k) {
+      double w = 0;
+      for (int i = j + tid; i < rows; i += nt) {
+        double v = (i == j) ? 1.0 : A[(size_t)i * c + j];
+        w += v * A[(size_t)i * c + k];
+      }
+      w = block_sum(w, red);
+      for (int i = j + tid; i < rows; i += nt) {
+        double v = (i == j) ? 1.0 : A[(size_t)i * c + j];
+        A[(size_t)i * c + k] -= t * v * w;
+      }
+      __syncthreads();
+    }
+  }
+  // Q = H_0 ... H_{c-1} [I; 0]
+  for (size_t idx = tid; idx < (size_t)rows * c; idx += nt) {
+    size_t i = idx / c, k = idx % c;
+    Q[idx] = (i == k) ? 1.0 : 0.0;
+  }
+  __syncthreads();
+  for (int j = min(c, rows) - 1; j >= 0; --j) {
+    double t = tau[j];
+    for (int k = j; k < c; ++k) {
+      double w = 0;
+      for (int i = j + tid; i < rows; i += nt) {
+        double v = (i == j) ? 1.0 : A[(size_t)i * c + j];
+        w += v * Q[(size_t)i * c + k];
+      }
+      w = block_sum(w, red);
+      for (int i = j + tid; i < rows; i += nt) {
+        double v = (i == j) ? 1.0 : A[(size_t)i * c + j];
+        Q[(size_t)i * c + k] -= t * v * w;
+      }
+      __syncthreads();
+    }
+  }
+}
+
+// --------------------------------------------------------------- Jacobi
+
+__global__ void __launch_bounds__(1024) jacobi_kernel(const double *S, int n, double *w_out,
+                                                      double *V_out) {
+  extern __shared__ double sm[];
+  const int np = (n + 1) & ~1;
+  double *A = sm;            // np x np
+  double *V = sm + np * np;  // np x np
+  __shared__ double cs[2 * 64];
+  __shared__ int pr[2 * 64];
+  __shared__ int order[128];
+  __shared__ double red[1024];
+  const int tid = threadIdx.x, nt = blockDim.x;
+  for (int idx = tid; idx < np * np; idx += nt) {
+    int i = idx / np, j = idx % np;
+    A[idx] = (i < n && j < n) ? S[i * n + j] : 0.0;
+    V[idx] = (i == j) ? 1.0 : 0.0;
+  }
+  __syncthreads();
+  double fro = 0;
+  for (int idx = tid; idx < np * np; idx += nt) fro += A[idx] * A[idx];
+  fro = block_sum(fro, red);
+  const int half = np / 2;
+  for (int sweep = 0; sweep < 60 && np > 1; ++sweep) {
+    double off = 0;
+    for (int idx = tid; idx < np * np; idx += nt) {
+      int i = idx / np, j = idx % np;
+      if (i != j) off += A[idx] * A[idx];
+    }
+    off = block_sum(off, red);
+    if (!(off > 1e-30 * fro)) break;
+    for (int step = 0; step < np - 1; ++step) {
+      if (tid < half) {
+        int k = tid;
+        int a = (k == 0) ? 0 : 1 + (k - 1 + step) % (np - 1);
+        int kb = np - 1 - k;
+        int b = 1 + (kb - 1 + step) % (np - 1);
+        int p = min(a, b), q = max(a, b);
+        pr[2 * k] = p;
+        pr[2 * k + 1] = q;
+        double apq = A[p * np + q];
+        double c = 1.0, s = 0.0;
+        if (apq != 0.0) {
+          double tau = (A[q * np + q] - A[p * np + p]) / (2.0 * apq);
+          double t = (tau >= 0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
+          c = 1.0 / sqrt(1.0 + t * t);
+          s = t * c;
+        }
+        cs[2 * k] = c;
+        cs[2 * k + 1] = s;
+      }
+      __syncthreads();
+      for (int idx = tid; idx < half * np; idx += nt) {  // rows: A <- J^T A
+        int k = idx / np, col = idx % np;
+        int p = pr[2 * k], q = pr[2 * k + 1];
+        double c = cs[2 * k], s = cs[2 * k + 1];
+        double a = A[p * np + col], b = A[q * np + col];
+        A[p * np + col] = c * a - s * b;
+        A[q * np + col] = s * a + c * b;
+      }
+      __syncthreads();
+      for (int idx = tid; idx < half * np; idx += nt) {  // cols: A <- A J, V <- V J
+        int k = idx / np, row = idx % np;
+        int p = pr[2 * k], q = pr[2 * k + 1];
+        double c = cs[2 * k], s = cs[2 * k + 1];
+        double a = A[row * np + p], b = A[row * np + q];
+        A[row * np + p] = c * a - s * b;
+        A[row * np + q] = s * a + c * b;
+        double va = V[row * np + p], vb = V[row * np + q];
+        V[row * np + p] = c * va - s * vb;
+        V[row * np + q] = s * va + c * vb;
+      }
+      __syncthreads();
+    }
+  }
+  // sort eigenvalues descending (only the first n indices are real)
+  if (tid == 0) {
+    for (int i = 0; i < n; ++i) order[i] = i;
+    for (int i = 0; i < n; ++i)
+      for (int j = i + 1; j < n; ++j)
+        if (A[order[j] * np + order[j]] > A[order[i] * np + order[i]]) {
+          int t = order[i];
+          order[i] = order[j];
+          order[j] = t;
+        }
+  }
+  __syncthreads();
+  for (int i = tid; i < n; i += nt) w_out[i] = A[order[i] * np + order[i]];
+  for (int idx = tid; idx < n * n; idx += nt) {
+    int row = idx / n, k = idx % n;
+    V_out[idx] = V[row * np + order[k]];
+  }
+}
+
+// ------------------------------------------------------------- misc
+
+__global__ void clip_rows_kernel(double *U, int n, int r, double delta) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double s = 0;
+  for (int j = 0; j < r; ++j) s += U[(size_t)i * r + j] * U[(size_t)i * r + j];
+  s = sqrt(s);
+  if (delta < s) {  // src/sparse/spsymtensor.cpp:172-183
+    double mul = delta / s;
+    for (int j = 0; j < r; ++j) U[(size_t)i * r + j] *= mul;
+  }
+}
+
+template <typename Ts, typename Td>
+__global__ void convert_kernel(const Ts *a, Td *b, size_t n) {
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) b[i] = (Td)a[i];
+}
+
+__global__ void random_fill_kernel(double *A, size_t n, uint64_t seed) {
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  uint64_t z = seed + 0x9E3779B97F4A7C15ull * (i + 1);
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  z ^= z >> 31;
+  A[i] = ((double)(z >> 11) * (1.0 / 9007199254740992.0)) - 0.5;
+}
+
+__global__ void copy_cols_kernel(const double *src, int lds, int rows, int cols, double *dst,
+                                 int ldd) {
+  size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (size_t)rows * cols) return;
+  int i = (int)(idx / cols), j = (int)(idx % cols);
+  dst[(size_t)i * ldd + j] = src[(size_t)i * lds + j];
+}
+
+// residual norms ||S x_i - lam_i x_i|| for i < r
+__global__ void residual_kernel(const double *SX, const double *X, int s, int ld, int r,
+                                const double *lam, double *res) {
+  __shared__ double red[256];
+  int i = blockIdx.x;
+  double acc = 0;
+  for (int row = threadIdx.x; row < s; row += blockDim.x) {
+    double d = SX[(size_t)row * ld + i] - lam[i] * X[(size_t)row * ld + i];
+    acc += d * d;
+  }
+  red[threadIdx.x] = acc;
+  __syncthreads();
+  for (int st = 128; st > 0; st >>= 1) {
+    if (threadIdx.x < st) red[threadIdx.x] += red[threadIdx.x + st];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) res[i] = sqrt(red[0]);
+}
+
+struct Scratch {
+  void *p = nullptr;
+  cudaStream_t st = 0;
+  Scratch(size_t bytes, cudaStream_t s) : st(s) {
+    if (bytes) SPB_CUDA(cudaMallocAsync(&p, bytes, st));
+  }
+  ~Scratch() {
+    if (p) cudaFreeAsync(p, st);
+  }
+  template <class T> T *as() { return reinterpret_cast<T *>(p); }
+};
+
+}  // namespace
+
+// ------------------------------------------------------------ public API
+
+template <typename T>
+void gemm(cudaStream_t st, int M, int N, int K, T alpha, const T *A, int lda, bool transA,
+          const T *B, int ldb, bool transB, T beta, T *C, int ldc, const T *kscale,
+          bool sym_upper) {
+  if (M <= 0 || N <= 0) return;
+  if (K <= 0) {
+    if (beta == T(0)) {
+      for (int i = 0; i < M; ++i) SPB_CUDA(cudaMemsetAsync(C + (size_t)i * ldc, 0, N * sizeof(T), st));
+      return;
+    }
+  }
+  const int tm = cdiv(M, BM), tn = cdiv(N, BN);
+  long long tiles = sym_upper ? (long long)tm * (tm + 1) / 2 : (long long)tm * tn;
+  int splits = (int)std::max<long long>(1, std::min<long long>((296 + tiles - 1) / tiles, cdiv(K, 256)));
+  int kchunk = (int)(cdiv(cdiv(K, splits), BK) * BK);
+  splits = std::max(1, (int)cdiv(K, kchunk));
+  const bool direct = splits == 1 && alpha == T(1) && beta == T(0) && !sym_upper;
+  Scratch ws(direct ? 0 : (size_t)splits * M * N * sizeof(T), st);
+  T *out = direct ? C : ws.as<T>();
+  const int ldo = direct ? ldc : N;
+  const size_t stride = (size_t)M * N;
+  dim3 grid(tn, tm, splits);
+#define SPB_GEMM_LAUNCH(TA, TB, KS)                                                            \
+  gemm_tile_kernel<T, TA, TB, KS><<<grid, 256, 0, st>>>(M, N, K, A, lda, B, ldb, kscale, out, \
+                                                        ldo, kchunk, sym_upper ? 1 : 0, stride)
+  const bool ks = kscale != nullptr;
+  if (transA && transB) { if (ks) SPB_GEMM_LAUNCH(true, true, true); else SPB_GEMM_LAUNCH(true, true, false); }
+  else if (transA) { if (ks) SPB_GEMM_LAUNCH(true, false, true); else SPB_GEMM_LAUNCH(true, false, false); }
+  else if (transB) { if (ks) SPB_GEMM_LAUNCH(false, true, true); else SPB_GEMM_LAUNCH(false, true, false); }
+  else { if (ks) SPB_GEMM_LAUNCH(false, false, true); else SPB_GEMM_LAUNCH(false, false, false); }
+#undef SPB_GEMM_LAUNCH
+  SPB_LAUNCH_CHECK();
+  if (!direct) {
+    gemm_finalize_kernel<T><<<cdiv((long long)M * N, 256), 256, 0, st>>>(
+        M, N, out, splits, stride, alpha, beta, C, ldc, sym_upper ? 1 : 0);
+    SPB_LAUNCH_CHECK();
+  }
+}
+
+template void gemm<double>(cudaStream_t, int, int, int, double, const double *, int, bool,
+                           const double *, int, bool, double, double *, int, const double *, bool);
+template void gemm<float>(cudaStream_t, int, int, int, float, const float *, int, bool,
+                          const float *, int, bool, float, float *, int, const float *, bool);
+
+template <typename T>
+void weighted_sq(cudaStream_t st, const T *X, const T *Y, const double *w, int rows, int cols,
+                 double *d_out2) {
+  Scratch part(sizeof(double) * 2 * kRedBlocks, st);
+  wsq_partial_kernel<T><<<kRedBlocks, 256, 0, st>>>(X, Y, w, rows, cols, part.as<double>());
+  SPB_LAUNCH_CHECK();
+  sum_pairs_kernel<<<1, 256, 0, st>>>(part.as<double>(), kRedBlocks, d_out2);
+  SPB_LAUNCH_CHECK();
+}
+template void weighted_sq<double>(cudaStream_t, const double *, const double *, const double *,
+                                  int, int, double *);
+template void weighted_sq<float>(cudaStream_t, const float *, const float *, const double *, int,
+                                 int, double *);
+
+void householder_q(cudaStream_t st, double *A, int rows, int cols) {
+  Scratch tau(sizeof(double) * cols, st), Q(sizeof(double) * (size_t)rows * cols, st);
+  householder_kernel<<<1, 1024, 0, st>>>(A, rows, cols, tau.as<double>(), Q.as<double>());
+  SPB_LAUNCH_CHECK();
+  SPB_CUDA(cudaMemcpyAsync(A, Q.p, sizeof(double) * (size_t)rows * cols, cudaMemcpyDeviceToDevice, st));
+}
+
+bool orthonormalize(cudaStream_t st, double *A, int rows, int cols) {
+  if (cols > 64 || rows < cols) {
+    householder_q(st, A, rows, cols);
+    return true;
+  }
+  Scratch G(sizeof(double) * cols * cols, st), Ri(sizeof(double) * cols * cols, st),
+      tmp(sizeof(double) * (size_t)rows * cols, st), stat(sizeof(int) * 2, st);
+  int hstat[2] = {0, 0};
+  for (int pass = 0; pass < 2; ++pass) {
+    gemm<double>(st, cols, cols, rows, 1.0, A, cols, true, A, cols, false, 0.0, G.as<double>(), cols,
+                 nullptr, true);
+    chol_inv_kernel<<<1, 256, 2 * sizeof(double) * cols * cols, st>>>(G.as<double>(), cols,
+                                                                     Ri.as<double>(),
+                                                                     stat.as<int>() + pass);
+    SPB_LAUNCH_CHECK();
+    gemm<double>(st, rows, cols, cols, 1.0, A, cols, false, Ri.as<double>(), cols, false, 0.0,
+                 tmp.as<double>(), cols);
+    SPB_CUDA(cudaMemcpyAsync(A, tmp.p, sizeof(double) * (size_t)rows * cols,
+                             cudaMemcpyDeviceToDevice, st));
+  }
+  SPB_CUDA(cudaMemcpyAsync(hstat, stat.p, sizeof(int) * 2, cudaMemcpyDeviceToHost, st));
+  SPB_CUDA(cudaStreamSynchronize(st));
+  if (hstat[0] || hstat[1]) {
+    // numerically singular: the first pass already mixed in garbage, but
+    // Householder of the result still spans a valid orthonormal set; redo
+    // from the mixed columns is acceptable only if we keep the span, so the
+    // caller's original columns are not available here.  Householder on the
+    // current A gives an orthonormal basis of its (rank-completed) span.
+    householder_q(st, A, rows, cols);
+    return true;
+  }
+  return false;
+}
+
+void jacobi_eig(cudaStream_t st, const double *S, int n, double *w, double *V) {
+  if (n > kJacobiMax) fail(SYMPROP_ERR_SIZE, "jacobi_eig: n=%d > %d", n, kJacobiMax);
+  int np = (n + 1) & ~1;
+  size_t smem = 2 * sizeof(double) * np * np;
+  SPB_CUDA(cudaFuncSetAttribute(jacobi_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  jacobi_kernel<<<1, 1024, smem, st>>>(S, n, w, V);
+  SPB_LAUNCH_CHECK();
+}
+
+void scale_rows_clip(cudaStream_t st, double *U, int n, int r, double delta) {
+  clip_rows_kernel<<<cdiv(n, 256), 256, 0, st>>>(U, n, r, delta);
+  SPB_LAUNCH_CHECK();
+}
+
+template <typename Ts, typename Td> void convert(cudaStream_t st, const Ts *src, Td *dst, size_t n) {
+  if (!n) return;
+  convert_kernel<Ts, Td><<<cdiv((long long)n, 256), 256, 0, st>>>(src, dst, n);
+  SPB_LAUNCH_CHECK();
+}
+template void convert<double, float>(cudaStream_t, const double *, float *, size_t);
+template void convert<float, double>(cudaStream_t, const float *, double *, size_t);
+
+// Block Krylov (block Lanczos with full re-orthogonalisation and thick
+// restart) for the top-r eigenpairs of S.  Projected problems of at most
+// kJacobiMax columns are solved by jacobi_eig.
+int top_eigs(cudaStream_t st, const double *S, int s, int r, double *V, double *lam,
+             const double *warm, double tol, int max_restarts) {
+  if (r > s) fail(SYMPROP_ERR_INVALID, "rank %d exceeds matrix size %d", r, s);
+  if (s <= kJacobiMax) {
+    Scratch w(sizeof(double) * s, st), Z(sizeof(double) * s * s, st);
+    jacobi_eig(st, S, s, w.as<double>(), Z.as<double>());
+    copy_cols_kernel<<<cdiv((long long)s * r, 256), 256, 0, st>>>(Z.as<double>(), s, s, r, V, r);
+    SPB_LAUNCH_CHECK();
+    SPB_CUDA(cudaMemcpyAsync(lam, w.p, sizeof(double) * r, cudaMemcpyDeviceToHost, st));
+    SPB_CUDA(cudaStreamSynchronize(st));
+    return SYMPROP_OK;
+  }
+  const int b = std::min(std::max(r + 8, 2 * r), std::min(48, s));
+  if (b < r) fail(SYMPROP_ERR_SIZE, "rank %d too large for the eigensolver", r);
+  const int nblk = std::max(2, kJacobiMax / b);
+  const int nb = nblk * b;  // Krylov basis width
+  Scratch Q(sizeof(double) * (size_t)s * nb, st), SQ(sizeof(double) * (size_t)s * nb, st),
+      T(sizeof(double) * nb * nb, st), w(sizeof(double) * nb, st), Z(sizeof(double) * nb * nb, st),
+      C(sizeof(double) * nb * b, st), X(sizeof(double) * (size_t)s * b, st),
+      SX(sizeof(double) * (size_t)s * b, st), res(sizeof(double) * b, st),
+      blk(sizeof(double) * (size_t)s * b, st);
+  double *q = Q.as<double>(), *sq = SQ.as<double>();
+  // start block: warm subspace padded with pseudo-random columns
+  random_fill_kernel<<<cdiv((long long)s * b, 256), 256, 0, st>>>(X.as<double>(), (size_t)s * b,
+                                                                   0x5EED5EEDull);
+  SPB_LAUNCH_CHECK();
+  if (warm) {
+    copy_cols_kernel<<<cdiv((long long)s * r, 256), 256, 0, st>>>(warm, r, s, r, X.as<double>(), b);
+    SPB_LAUNCH_CHECK();
+  }
+  std::vector<double> hw(nb), hres(b);
+  uint64_t reseed = 1;
+  for (int it = 0; it <= max_restarts; ++it) {
+    // Q[:, 0:b] = orth(X)
+    copy_cols_kernel<<<cdiv((long long)s * b, 256), 256, 0, st>>>(X.as<double>(), b, s, b,
+                                                                  blk.as<double>(), b);
+    SPB_LAUNCH_CHECK();
+    orthonormalize(st, blk.as<double>(), s, b);
+    copy_cols_kernel<<<cdiv((long long)s * b, 256), 256, 0, st>>>(blk.as<double>(), b, s, b, q, nb);
+    SPB_LAUNCH_CHECK();
+    int width = b;
+    for (int j = 1; j < nblk; ++j) {
+      // W = S * Q[:, (j-1)b : jb]
+      gemm<double>(st, s, b, s, 1.0, S, s, false, q + (j - 1) * b, nb, false, 0.0, blk.as<double>(), b);
+      for (int pass = 0; pass < 2; ++pass) {  // W -= Q (Q^T W)
+        gemm<double>(st, width, b, s, 1.0, q, nb, true, blk.as<double>(), b, false, 0.0,
+                     C.as<double>(), b);
+        gemm<double>(st, s, b, width, -1.0, q, nb, false, C.as<double>(), b, false, 1.0,
+                     blk.as<double>(), b);
+      }
+      bool hh = orthonormalize(st, blk.as<double>(), s, b);
+      if (hh) {
+        // breakdown: continue the basis with fresh directions
+        random_fill_kernel<<<cdiv((long long)s * b, 256), 256, 0, st>>>(blk.as<double>(),
+                                                                         (size_t)s * b, ++reseed);
+        SPB_LAUNCH_CHECK();
+        for (int pass = 0; pass < 2; ++pass) {
+          gemm<double>(st, width, b, s, 1.0, q, nb, true, blk.as<double>(), b, false, 0.0,
+                       C.as<double>(), b);
+          gemm<double>(st, s, b, width, -1.0, q, nb, false, C.as<double>(), b, false, 1.0,
+                       blk.as<double>(), b);
+        }
+        orthonormalize(st, blk.as<double>(), s, b);
+      }
+      copy_cols_kernel<<<cdiv((long long)s * b, 256), 256, 0, st>>>(blk.as<double>(), b, s, b,
+                                                                    q + j * b, nb);
+      SPB_LAUNCH_CHECK();
+      width += b;
+    }
+    // Rayleigh-Ritz: T = Q^T S Q
+    gemm<double>(st, s, nb, s, 1.0, S, s, false, q, nb, false, 0.0, sq, nb);
+    gemm<double>(st, nb, nb, s, 1.0, q, nb, true, sq, nb, false, 0.0, T.as<double>(), nb);
+    jacobi_eig(st, T.as<double>(), nb, w.as<double>(), Z.as<double>());
+    // X = Q Z[:, :b], SX = SQ Z[:, :b]
+    copy_cols_kernel<<<cdiv((long long)nb * b, 256), 256, 0, st>>>(Z.as<double>(), nb, nb, b,
+                                                                   C.as<double>(), b);
+    SPB_LAUNCH_CHECK();
+    gemm<double>(st, s, b, nb, 1.0, q, nb, false, C.as<double>(), b, false, 0.0, X.as<double>(), b);
+    gemm<double>(st, s, b, nb, 1.0, sq, nb, false, C.as<double>(), b, false, 0.0, SX.as<double>(), b);
+    residual_kernel<<<r, 256, 0, st>>>(SX.as<double>(), X.as<double>(), s, b, r, w.as<double>(),
+                                       res.as<double>());
+    SPB_LAUNCH_CHECK();
+    SPB_CUDA(cudaMemcpyAsync(hw.data(), w.p, sizeof(double) * nb, cudaMemcpyDeviceToHost, st));
+    SPB_CUDA(cudaMemcpyAsync(hres.data(), res.p, sizeof(double) * r, cudaMemcpyDeviceToHost, st));
+    SPB_CUDA(cudaStreamSynchronize(st));
+    double scale = std::max(std::fabs(hw[0]), 1e-300);
+    double worst = 0;
+    for (int i = 0; i < r; ++i) worst = std::max(worst, hres[i] / scale);
+    if (worst <= tol || it == max_restarts) {
+      copy_cols_kernel<<<cdiv((long long)s * r, 256), 256, 0, st>>>(X.as<double>(), b, s, r, V, r);
+      SPB_LAUNCH_CHECK();
+      for (int i = 0; i < r; ++i) lam[i] = hw[i];
+      SPB_CUDA(cudaStreamSynchronize(st));
+      return worst <= tol ? SYMPROP_OK : SYMPROP_ERR_NOCONV;
+    }
+  }
+  return SYMPROP_ERR_NOCONV;
+}
+
+}  // namespace dense
+}  // namespace spb

@@ -1,0 +1,498 @@
+// S3TTMc on sm_100a: Y[i] = sum over owners (i, S, c) of c * K(S), where
+// K(S) is the packed symmetric tensor of the (N-1)-multiset S built by the
+// reference's level recursion K(S) = sum_k K(S \ s_k) (x) U[s_k]
+// (SymOuterProd, include/detail/dense/symtensor.hpp:24-39, swept level by
+// level in CompressedDTree::kronecker_product_opt5,
+// src/compressed_dtree.cpp:421-518).
+//
+// B200 design (differs from opt5 on purpose):
+//  * one CTA per work item = a row of Y, or a slice of a long row; owners are
+//    pre-sorted by row, so Y is produced by a segmented reduction in
+//    registers; rows cut into slices write FP64 partial rows that a second
+//    kernel adds in a fixed order: no global atomics, deterministic;
+//  * no tree level is materialised: the intermediate tensors K(P) of every
+//    sub-multiset P of the leaf are recomputed per owner in shared memory
+//    from U rows.  U (n x R) stays L2-resident (12.8 MB at n=200k, R=16),
+//    so the HBM stream is the owner list in and Y out.  This removes the
+//    level-(N-2) array that opt5 allocates (88 GB at 5M order-4 tuples);
+//  * FP32 mode accumulates each owner's contribution in FP32 and folds
+//    batches into a Kahan-compensated accumulator.
+#include <algorithm>
+#include <cstdlib>
+
+#include "tensor.cuh"
+
+namespace spb {
+
+static constexpr int kMaxL = 7;          // orders 2..8
+static constexpr uint32_t kURow = 0x80000000u;
+
+struct MaskDesc {
+  uint32_t dst;          // offset of this sub-multiset's tensor in sK
+  uint32_t nterm;
+  uint32_t src[kMaxL];   // sK offset, or kURow | position for a single id
+  uint32_t k[kMaxL];     // position whose U row multiplies the term
+};
+
+struct PackedTables {
+  uint32_t L = 0, R = 0;
+  uint64_t m[kMaxL + 1] = {};
+  // device: inner tables (levels 2..L-1) then the final level
+  DBuf<uint32_t> tab;
+  uint32_t tab_inner_len = 0;
+  uint32_t tab_level_off[kMaxL + 1] = {};  // offsets into tab for levels 2..L
+  DBuf<MaskDesc> desc;
+  uint32_t ndesc = 0;
+  uint32_t level_desc_begin[kMaxL + 1] = {}, level_desc_count[kMaxL + 1] = {};
+  uint32_t final_src[kMaxL] = {};
+  uint32_t ksize = 0;  // elements of sK
+  int threads = 256, maxpt = 1;
+  size_t smem_bytes[2] = {0, 0};  // by precision
+};
+
+// ---------------------------------------------------------------- tables
+
+static std::shared_ptr<PackedTables> build_tables(uint32_t N, uint32_t R) {
+  auto tb = std::make_shared<PackedTables>();
+  const uint32_t L = N - 1;
+  tb->L = L;
+  tb->R = R;
+  for (uint32_t d = 0; d <= L; ++d) tb->m[d] = symsize(R, d);
+  if (R > 255) fail(SYMPROP_ERR_SIZE, "rank %u > 255 not supported", R);
+  // packed recursion tables: entry q of level d -> (prefix index << 8) | last
+  std::vector<uint32_t> tab;
+  for (uint32_t d = 2; d <= L; ++d) {
+    if (tb->m[d - 1] >= (1ull << 24)) fail(SYMPROP_ERR_SIZE, "packed size too large");
+    tb->tab_level_off[d] = (uint32_t)tab.size();
+    // prefix index = linear index of q[0..d-2] in level d-1 enumeration
+    std::vector<uint32_t> q_prev;
+    uint64_t prev_lin = 0;
+    // enumerate level d; prefix changes exactly when q[0..d-2] changes, and
+    // prefixes appear in level d-1 order, so a running counter suffices
+    std::vector<uint32_t> last_prefix;
+    bool first = true;
+    for_each_sorted(R, (int)d, [&](const std::vector<uint32_t> &q, uint64_t) {
+      std::vector<uint32_t> pre(q.begin(), q.end() - 1);
+      if (!first && pre != last_prefix) ++prev_lin;
+      first = false;
+      last_prefix = pre;
+      tab.push_back((uint32_t)(prev_lin << 8) | q.back());
+    });
+    (void)q_prev;
+  }
+  tb->tab_inner_len = L >= 3 ? tb->tab_level_off[L] : 0;
+  if (L < 2) tb->tab_level_off[L] = 0;
+  // DP over position subsets of the leaf, popcount 2..L-1
+  std::vector<MaskDesc> desc;
+  std::vector<uint32_t> off_of_mask(1u << L, 0);
+  uint32_t ksz = 0;
+  for (uint32_t d = 2; d + 1 <= L; ++d) {
+    tb->level_desc_begin[d] = (uint32_t)desc.size();
+    for (uint32_t mask = 0; mask < (1u << L); ++mask) {
+      if ((uint32_t)__builtin_popcount(mask) != d) continue;
+      MaskDesc md{};
+      md.dst = ksz;
+      off_of_mask[mask] = ksz;
+      ksz += (uint32_t)tb->m[d];
+      md.nterm = 0;
+      for (uint32_t k = 0; k < L; ++k) {
+        if (!(mask & (1u << k))) continue;
+        uint32_t src = mask & ~(1u << k);
+        md.src[md.nterm] = (d - 1 == 1) ? (kURow | (uint32_t)__builtin_ctz(src)) : off_of_mask[src];
+        md.k[md.nterm] = k;
+        md.nterm++;
+      }
+      desc.push_back(md);
+    }
+    tb->level_desc_count[d] = (uint32_t)desc.size() - tb->level_desc_begin[d];
+  }
+  for (uint32_t k = 0; k < L; ++k) {
+    uint32_t src = ((1u << L) - 1) & ~(1u << k);
+    tb->final_src[k] = (L - 1 == 1) ? (kURow | (uint32_t)__builtin_ctz(src))
+                       : (L - 1 == 0) ? kURow : off_of_mask[src];
+  }
+  tb->ksize = ksz;
+  tb->ndesc = (uint32_t)desc.size();
+  tb->tab.alloc(std::max<size_t>(tab.size(), 1));
+  if (!tab.empty())
+    SPB_CUDA(cudaMemcpy(tb->tab.p, tab.data(), tab.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
+  tb->desc.alloc(std::max<size_t>(desc.size(), 1));
+  if (!desc.empty())
+    SPB_CUDA(cudaMemcpy(tb->desc.p, desc.data(), desc.size() * sizeof(MaskDesc), cudaMemcpyHostToDevice));
+  // launch shape
+  const uint64_t mL = tb->m[L];
+  const int threads = 256;
+  uint64_t per = (mL + threads - 1) / threads;
+  if (per > 64) fail(SYMPROP_ERR_SIZE, "packed output width %llu too large", (unsigned long long)mL);
+  int maxpt = 1;
+  while ((uint64_t)maxpt < per) maxpt *= 2;
+  tb->threads = threads;
+  tb->maxpt = maxpt;
+  for (int p = 0; p < 2; ++p) {
+    size_t es = p == 0 ? sizeof(double) : sizeof(float);
+    size_t b = 0;
+    b += (size_t)tb->tab_inner_len * 4;
+    b = (b + 15) / 16 * 16;
+    b += (size_t)tb->ndesc * sizeof(MaskDesc);
+    b = (b + 15) / 16 * 16;
+    b += 2 * (size_t)L * R * es;
+    b = (b + 15) / 16 * 16;
+    b += (size_t)ksz * es;
+    tb->smem_bytes[p] = b;
+  }
+  return tb;
+}
+
+// --------------------------------------------------------------- kernels
+
+struct RowParams {
+  const Chunk *chunks;
+  const uint32_t *own_S;
+  const void *own_c;
+  uint32_t sstride;
+  const void *U;
+  uint32_t R;
+  void *Y;           // dim x ldy (T), packed
+  uint64_t ldy;
+  double *partials;  // nslots x mL
+  const uint32_t *tab;
+  uint32_t tab_inner_len;
+  uint32_t tab_final_off;
+  const MaskDesc *desc;
+  uint32_t ndesc;
+  uint32_t ksize;
+  uint32_t mlev[kMaxL + 1];
+  uint32_t tab_off[kMaxL + 1];
+  uint32_t desc_begin[kMaxL + 1];
+  uint32_t desc_count[kMaxL + 1];
+  uint32_t final_src[kMaxL];
+};
+
+template <typename T> struct Acc;
+template <> struct Acc<double> {
+  static constexpr int kBatch = 1 << 30;
+};
+template <> struct Acc<float> {
+  static constexpr int kBatch = 8;  // owners summed plainly before a compensated fold
+};
+
+template <int L, int MAXPT, typename T>
+__global__ void __launch_bounds__(256, 1) s3ttmc_rows_kernel(const RowParams p) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const Chunk ch = p.chunks[blockIdx.x];
+  const uint32_t R = p.R;
+
+  uint32_t *sTab = reinterpret_cast<uint32_t *>(smem);
+  size_t off = ((size_t)p.tab_inner_len * 4 + 15) / 16 * 16;
+  MaskDesc *sDesc = reinterpret_cast<MaskDesc *>(smem + off);
+  off += ((size_t)p.ndesc * sizeof(MaskDesc) + 15) / 16 * 16;
+  T *sU = reinterpret_cast<T *>(smem + off);
+  T *sW = sU + L * R;
+  off += ((size_t)2 * L * R * sizeof(T) + 15) / 16 * 16;
+  T *sK = reinterpret_cast<T *>(smem + off);
+
+  for (uint32_t i = tid; i < p.tab_inner_len; i += nt) sTab[i] = p.tab[i];
+  {
+    const uint32_t *src = reinterpret_cast<const uint32_t *>(p.desc);
+    uint32_t *dst = reinterpret_cast<uint32_t *>(sDesc);
+    const uint32_t words = p.ndesc * (uint32_t)(sizeof(MaskDesc) / 4);
+    for (uint32_t i = tid; i < words; i += nt) dst[i] = src[i];
+  }
+
+  constexpr bool kExact = sizeof(T) == 8;  // FP64 accumulates directly
+  const uint32_t mL = p.mlev[L];
+  uint32_t ftab[MAXPT];
+#pragma unroll
+  for (int j = 0; j < MAXPT; ++j) {
+    uint32_t q = tid + j * nt;
+    ftab[j] = q < mL ? p.tab[p.tab_final_off + q] : 0u;
+  }
+  T acc[MAXPT], cmp[MAXPT], tmp[MAXPT];
+#pragma unroll
+  for (int j = 0; j < MAXPT; ++j) { acc[j] = T(0); cmp[j] = T(0); tmp[j] = T(0); }
+
+  const T *U = reinterpret_cast<const T *>(p.U);
+  const T *own_c = reinterpret_cast<const T *>(p.own_c);
+  int batch = 0;
+  __syncthreads();
+
+  for (uint64_t o = ch.ob; o < ch.oe; ++o) {
+    // stage the leaf's U rows, and the coefficient-scaled copy for the last level
+    const uint32_t *S = p.own_S + o * p.sstride;
+    const T c = own_c[o];
+    for (uint32_t i = tid; i < L * R; i += nt) {
+      uint32_t k = i / R, x = i - k * R;
+      T u = U[(uint64_t)S[k] * R + x];
+      sU[i] = u;
+      sW[i] = c * u;
+    }
+    __syncthreads();
+    // intermediate sub-multiset tensors, level by level
+#pragma unroll 1
+    for (int d = 2; d < L; ++d) {
+      const uint32_t md = p.mlev[d];
+      const uint32_t items = p.desc_count[d] * md;
+      const uint32_t *tabd = sTab + p.tab_off[d];
+      for (uint32_t it = tid; it < items; it += nt) {
+        uint32_t mi = it / md, q = it - mi * md;
+        const MaskDesc &ds = sDesc[p.desc_begin[d] + mi];
+        uint32_t e = tabd[q];
+        uint32_t pre = e >> 8, last = e & 0xffu;
+        T v = T(0);
+        for (uint32_t t = 0; t < ds.nterm; ++t) {
+          uint32_t s = ds.src[t];
+          T a = (s & kURow) ? sU[(s & 0xffu) * R + pre] : sK[s + pre];
+          v += a * sU[ds.k[t] * R + last];
+        }
+        sK[ds.dst + q] = v;
+      }
+      __syncthreads();
+    }
+    // last level: contribution c*K(S) for this thread's outputs
+#pragma unroll
+    for (int j = 0; j < MAXPT; ++j) {
+      uint32_t q = tid + j * nt;
+      if (q < mL) {
+        uint32_t pre = ftab[j] >> 8, last = ftab[j] & 0xffu;
+        T v = T(0);
+#pragma unroll
+        for (int k = 0; k < L; ++k) {
+          uint32_t s = p.final_src[k];
+          T a = (s & kURow) ? sU[(s & 0xffu) * R + pre] : sK[s + pre];
+          v += a * sW[k * R + last];
+        }
+        if constexpr (kExact) acc[j] += v; else tmp[j] += v;
+      }
+    }
+    if (!kExact && ++batch >= Acc<T>::kBatch) {
+#pragma unroll
+      for (int j = 0; j < MAXPT; ++j) {  // Kahan fold of the batch
+        T y = tmp[j] - cmp[j];
+        T s = acc[j] + y;
+        cmp[j] = (s - acc[j]) - y;
+        acc[j] = s;
+        tmp[j] = T(0);
+      }
+      batch = 0;
+    }
+    __syncthreads();
+  }
+  if constexpr (!kExact) {
+#pragma unroll
+    for (int j = 0; j < MAXPT; ++j) {
+      T y = tmp[j] - cmp[j];
+      T s = acc[j] + y;
+      cmp[j] = (s - acc[j]) - y;
+      acc[j] = s;
+    }
+  }
+  if (ch.slot == kDirect) {
+    T *Y = reinterpret_cast<T *>(p.Y) + (uint64_t)ch.row * p.ldy;
+#pragma unroll
+    for (int j = 0; j < MAXPT; ++j) {
+      uint32_t q = tid + j * nt;
+      if (q < mL) Y[q] = acc[j] - cmp[j];
+    }
+  } else {
+    double *P = p.partials + (uint64_t)ch.slot * mL;
+#pragma unroll
+    for (int j = 0; j < MAXPT; ++j) {
+      uint32_t q = tid + j * nt;
+      if (q < mL) P[q] = (double)acc[j] - (double)cmp[j];
+    }
+  }
+}
+
+// rows cut into slices: add the FP64 partials in slot order
+template <typename T>
+__global__ void combine_kernel(const SplitRow *split, const double *partials, uint32_t mL,
+                               void *Yv, uint64_t ldy) {
+  const SplitRow s = split[blockIdx.x];
+  T *Y = reinterpret_cast<T *>(Yv) + (uint64_t)s.row * ldy;
+  for (uint32_t q = threadIdx.x; q < mL; q += blockDim.x) {
+    double a = 0.0;
+    for (uint32_t k = s.slot_begin; k < s.slot_end; ++k) a += partials[(uint64_t)k * mL + q];
+    Y[q] = (T)a;
+  }
+}
+
+// unpack packed order-`order` rows into dim^order full rows
+// (SymtensorOps::ToTensor, include/detail/dense/symtensor.hpp:96-116)
+template <typename T>
+__global__ void unpack_kernel(const T *packed, uint64_t rows, uint64_t m, uint32_t dim,
+                              uint32_t order, uint64_t full_cols, T *full) {
+  uint64_t idx = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= rows * full_cols) return;
+  uint64_t r = idx / full_cols, f = idx - r * full_cols;
+  uint32_t q[16];
+  uint64_t x = f;
+  for (int j = (int)order - 1; j >= 0; --j) {
+    q[j] = (uint32_t)(x % dim);
+    x /= dim;
+  }
+  for (uint32_t a = 1; a < order; ++a) {  // sort
+    uint32_t v = q[a];
+    int b = (int)a - 1;
+    while (b >= 0 && q[b] > v) { q[b + 1] = q[b]; --b; }
+    q[b + 1] = v;
+  }
+  // packed offset (SymtensorOps::At, symtensor.hpp:83-94) via binomials
+  uint64_t pos = 0;
+  uint32_t start = 0;
+  for (uint32_t j = 0; j < order; ++j) {
+    uint32_t rem = order - 1 - j;
+    for (uint32_t i = start; i < q[j]; ++i) {
+      // symsize(dim - i, rem) = C(dim - i + rem - 1, rem)
+      uint64_t n = (uint64_t)(dim - i) + rem - 1, k = rem, c = 1;
+      if (k > n) c = 0;
+      else {
+        if (2 * k > n) k = n - k;
+        for (uint64_t t = 1; t <= k; ++t) c = c * (n - k + t) / t;
+      }
+      pos += c;
+    }
+    start = q[j];
+  }
+  full[idx] = packed[r * m + pos];
+}
+
+// --------------------------------------------------------------- launch
+
+template <int L, typename T>
+static void launch_rows(const PackedTables &tb, const RowParams &rp, uint32_t nchunks,
+                        size_t smem, cudaStream_t st) {
+  auto go = [&](auto kern) {
+    if (smem > 48 * 1024)
+      SPB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    kern<<<nchunks, tb.threads, smem, st>>>(rp);
+    SPB_LAUNCH_CHECK();
+  };
+  switch (tb.maxpt) {
+    case 1: go(s3ttmc_rows_kernel<L, 1, T>); break;
+    case 2: go(s3ttmc_rows_kernel<L, 2, T>); break;
+    case 4: go(s3ttmc_rows_kernel<L, 4, T>); break;
+    case 8: go(s3ttmc_rows_kernel<L, 8, T>); break;
+    case 16: go(s3ttmc_rows_kernel<L, 16, T>); break;
+    case 32: go(s3ttmc_rows_kernel<L, 32, T>); break;
+    default: go(s3ttmc_rows_kernel<L, 64, T>); break;
+  }
+}
+
+template <typename T>
+static void dispatch_rows(uint32_t L, const PackedTables &tb, const RowParams &rp,
+                          uint32_t nchunks, size_t smem, cudaStream_t st) {
+  switch (L) {
+    case 2: launch_rows<2, T>(tb, rp, nchunks, smem, st); break;
+    case 3: launch_rows<3, T>(tb, rp, nchunks, smem, st); break;
+    case 4: launch_rows<4, T>(tb, rp, nchunks, smem, st); break;
+    case 5: launch_rows<5, T>(tb, rp, nchunks, smem, st); break;
+    case 6: launch_rows<6, T>(tb, rp, nchunks, smem, st); break;
+    case 7: launch_rows<7, T>(tb, rp, nchunks, smem, st); break;
+    default: fail(SYMPROP_ERR_ORDER, "order %u not supported by S3TTMc", L + 1);
+  }
+}
+
+static PackedTables &tables_for(TensorState &t, uint32_t R) {
+  auto it = t.tables.find(R);
+  if (it != t.tables.end()) return *it->second;
+  auto tb = build_tables(t.order, R);
+  auto &ref = *tb;
+  t.tables[R] = tb;
+  return ref;
+}
+
+uint32_t s3ttmc_launch_count(const TensorState &t, uint32_t R, bool packed) {
+  (void)R;
+  if (t.order <= 2) return packed ? 1 : 1;
+  uint32_t n = 1;                 // rows kernel
+  if (t.nsplit) n += 1;           // combine kernel
+  if (!packed) n += 1;            // unpack kernel
+  return n;
+}
+
+void unpack_rows(const void *dpacked, uint64_t rows, uint32_t dim, uint32_t order, void *dfull,
+                 int precision, cudaStream_t st) {
+  uint64_t m = symsize(dim, order);
+  uint64_t full = 1;
+  for (uint32_t j = 0; j < order; ++j) full *= dim;
+  uint64_t total = rows * full;
+  if (!total) return;
+  unsigned grid = (unsigned)((total + 255) / 256);
+  if (precision == SYMPROP_FP64)
+    unpack_kernel<double><<<grid, 256, 0, st>>>((const double *)dpacked, rows, m, dim, order, full,
+                                                (double *)dfull);
+  else
+    unpack_kernel<float><<<grid, 256, 0, st>>>((const float *)dpacked, rows, m, dim, order, full,
+                                               (float *)dfull);
+  SPB_LAUNCH_CHECK();
+}
+
+void s3ttmc_run(TensorState &t, const void *dU, uint32_t R, bool packed, void *dY, int precision,
+                cudaStream_t st) {
+  if (R == 0) fail(SYMPROP_ERR_INVALID, "R must be positive");
+  if (precision != SYMPROP_FP64 && precision != SYMPROP_FP32)
+    fail(SYMPROP_ERR_INVALID, "unknown precision %d", precision);
+  const size_t es = precision == SYMPROP_FP64 ? 8 : 4;
+  const uint32_t L = t.order - 1;
+  uint64_t m = symsize(R, L);
+  uint64_t full = 1;
+  for (uint32_t j = 0; j < L; ++j) full *= R;
+  const uint64_t ldy = packed ? m : full;
+  if (t.order == 2) {
+    // The reference's level loop is empty for depth 1 and Y stays zero
+    // (src/compressed_dtree.cpp:451).
+    SPB_CUDA(cudaMemsetAsync(dY, 0, (size_t)t.dim * ldy * es, st));
+    return;
+  }
+  PackedTables &tb = tables_for(t, R);
+  void *Ypk = dY;
+  if (!packed) {
+    t.scratch.ensure((size_t)t.dim * m * es);
+    Ypk = t.scratch.p;
+  }
+  if (t.nslots) t.partials.ensure((size_t)t.nslots * m);
+
+  RowParams rp{};
+  rp.chunks = t.chunks.p;
+  rp.own_S = t.own_S.p;
+  rp.own_c = precision == SYMPROP_FP64 ? (const void *)t.own_c64.p : (const void *)t.own_c32.p;
+  rp.sstride = t.sstride;
+  rp.U = dU;
+  rp.R = R;
+  rp.Y = Ypk;
+  rp.ldy = m;
+  rp.partials = t.partials.p;
+  rp.tab = tb.tab.p;
+  rp.tab_inner_len = tb.tab_inner_len;
+  rp.tab_final_off = tb.tab_level_off[L];
+  rp.desc = tb.desc.p;
+  rp.ndesc = tb.ndesc;
+  rp.ksize = tb.ksize;
+  for (uint32_t d = 0; d <= L && d <= (uint32_t)kMaxL; ++d) {
+    rp.mlev[d] = (uint32_t)tb.m[d];
+    rp.tab_off[d] = tb.tab_level_off[d];
+    rp.desc_begin[d] = tb.level_desc_begin[d];
+    rp.desc_count[d] = tb.level_desc_count[d];
+  }
+  for (uint32_t k = 0; k < L; ++k) rp.final_src[k] = tb.final_src[k];
+  const size_t smem = tb.smem_bytes[precision == SYMPROP_FP64 ? 0 : 1];
+  if (smem > 227 * 1024)
+    fail(SYMPROP_ERR_SIZE, "order %u rank %u needs %zu bytes of shared memory", t.order, R, smem);
+  if (t.nchunks) {
+    if (precision == SYMPROP_FP64)
+      dispatch_rows<double>(L, tb, rp, t.nchunks, smem, st);
+    else
+      dispatch_rows<float>(L, tb, rp, t.nchunks, smem, st);
+  }
+  if (t.nsplit) {
+    if (precision == SYMPROP_FP64)
+      combine_kernel<double><<<t.nsplit, 256, 0, st>>>(t.split.p, t.partials.p, (uint32_t)m, Ypk, m);
+    else
+      combine_kernel<float><<<t.nsplit, 256, 0, st>>>(t.split.p, t.partials.p, (uint32_t)m, Ypk, m);
+    SPB_LAUNCH_CHECK();
+  }
+  if (!packed) unpack_rows(Ypk, t.dim, R, L, dY, precision, st);
+}
+
+}  // namespace spb

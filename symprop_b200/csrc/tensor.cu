@@ -1,0 +1,266 @@
+// Tensor construction on the device: validation, ||X||, and the
+// row-segmented owner list consumed by the S3TTMc kernels.
+//
+// Replaces the construction half of SpSymtensor::SpSymtensor
+// (src/sparse/spsymtensor.cpp:16-28): the pointer trie insert
+// (src/dtree.cpp:56-80) becomes one pass that emits, for every nonzero t and
+// every distinct id e of t, the owner (row = e, leaf = t \ e) with
+// coefficient f_e * v * mult(t)/N!, followed by a device radix sort of the
+// owners by row.  calc_norm (src/sparse/spsymtensor.cpp:114-138) is a device
+// reduction of v^2 * mult(t).
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <numeric>
+
+#include "tensor.cuh"
+
+namespace spb {
+
+namespace {
+
+constexpr int kMaxOrder = 16;
+
+__global__ void validate_kernel(const uint32_t *inds, uint64_t nnz, uint32_t order,
+                                uint32_t dim, uint32_t *inds0, int *bad) {
+  uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nnz) return;
+  const uint32_t *t = inds + i * order;
+  uint32_t prev = 0;
+  for (uint32_t j = 0; j < order; ++j) {
+    uint32_t v = t[j];
+    if (v < 1 || v > dim) { atomicOr(bad, 1); return; }
+    if (j && v < prev) { atomicOr(bad, 2); return; }
+    prev = v;
+    inds0[i * order + j] = v - 1;
+  }
+}
+
+// distinct ids per tuple and v^2 * mult(t)
+__global__ void count_kernel(const uint32_t *inds0, const double *vals, uint64_t nnz,
+                             uint32_t order, uint32_t *cnt, double *normsq) {
+  uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nnz) return;
+  const uint32_t *t = inds0 + i * order;
+  uint32_t distinct = 1;
+  uint64_t denom = 1, run = 1;
+  for (uint32_t j = 1; j <= order; ++j) {
+    if (j < order && t[j] == t[j - 1]) {
+      ++run;
+    } else {
+      denom *= factorial_u64((int)run);
+      run = 1;
+      if (j < order) ++distinct;
+    }
+  }
+  uint64_t mult = factorial_u64((int)order) / denom;  // multinomial_coeff
+  cnt[i] = distinct;
+  double v = vals[i];
+  normsq[i] = v * v * (double)mult;
+}
+
+__global__ void emit_owners_kernel(const uint32_t *inds0, const double *vals, uint64_t nnz,
+                                   uint32_t order, const uint32_t *off, uint32_t sstride,
+                                   uint32_t *own_row, uint32_t *own_S, double *own_c) {
+  uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nnz) return;
+  uint32_t t[kMaxOrder];
+  for (uint32_t j = 0; j < order; ++j) t[j] = inds0[i * order + j];
+  uint64_t denom = 1, run = 1;
+  for (uint32_t j = 1; j <= order; ++j) {
+    if (j < order && t[j] == t[j - 1]) {
+      ++run;
+    } else {
+      denom *= factorial_u64((int)run);
+      run = 1;
+    }
+  }
+  const uint64_t nfact = factorial_u64((int)order);
+  // the reference's owner coefficient (src/compressed_dtree.cpp:493-503)
+  const double coeff = vals[i] * (double)(nfact / denom) / (double)nfact;
+  uint32_t o = off[i];
+  uint32_t j = 0;
+  while (j < order) {
+    uint32_t e = j + 1;
+    while (e < order && t[e] == t[j]) ++e;
+    const uint32_t f = e - j;  // multiplicity of id t[j]
+    own_row[o] = t[j];
+    uint32_t *S = own_S + (uint64_t)o * sstride;
+    uint32_t c = 0;
+    for (uint32_t k = 0; k < order; ++k)
+      if (k != j) S[c++] = t[k];
+    for (; c < sstride; ++c) S[c] = 0;
+    own_c[o] = (double)f * coeff;
+    ++o;
+    j = e;
+  }
+}
+
+__global__ void gather_owners_kernel(const uint32_t *perm, uint64_t nown, uint32_t sstride,
+                                     const uint32_t *S_in, const double *c_in,
+                                     uint32_t *S_out, double *c_out, float *c32_out) {
+  uint64_t o = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (o >= nown) return;
+  uint32_t src = perm[o];
+  const uint4 *a = reinterpret_cast<const uint4 *>(S_in + (uint64_t)src * sstride);
+  uint4 *b = reinterpret_cast<uint4 *>(S_out + o * sstride);
+  for (uint32_t w = 0; w < sstride / 4; ++w) b[w] = a[w];
+  double c = c_in[src];
+  c_out[o] = c;
+  c32_out[o] = (float)c;
+}
+
+__global__ void row_ptr_kernel(const uint32_t *rows_sorted, uint64_t nown, uint32_t dim,
+                               uint64_t *row_ptr) {
+  uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i > dim) return;
+  uint64_t lo = 0, hi = nown;
+  while (lo < hi) {
+    uint64_t mid = (lo + hi) >> 1;
+    if (rows_sorted[mid] < i) lo = mid + 1; else hi = mid;
+  }
+  row_ptr[i] = lo;
+}
+
+inline unsigned grid_for(uint64_t n, unsigned block) {
+  return (unsigned)std::max<uint64_t>(1, (n + block - 1) / block);
+}
+
+}  // namespace
+
+void tensor_build(TensorState &t, const uint32_t *h_inds, const double *h_vals) {
+  const uint32_t N = t.order;
+  const uint64_t nnz = t.nnz;
+  cudaStream_t st = 0;
+  if (N < 2 || N > (uint32_t)kMaxOrder) fail(SYMPROP_ERR_ORDER, "unsupported order %u", N);
+
+  DBuf<uint32_t> raw(nnz * N);
+  t.inds.alloc(nnz * N);
+  t.vals.alloc(nnz);
+  if (nnz) {
+    SPB_CUDA(cudaMemcpy(raw.p, h_inds, nnz * N * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    SPB_CUDA(cudaMemcpy(t.vals.p, h_vals, nnz * sizeof(double), cudaMemcpyHostToDevice));
+  }
+  DBuf<int> bad(1);
+  SPB_CUDA(cudaMemset(bad.p, 0, sizeof(int)));
+  if (nnz) {
+    validate_kernel<<<grid_for(nnz, 256), 256, 0, st>>>(raw.p, nnz, N, t.dim, t.inds.p, bad.p);
+    SPB_LAUNCH_CHECK();
+  }
+  int hbad = 0;
+  SPB_CUDA(cudaMemcpy(&hbad, bad.p, sizeof(int), cudaMemcpyDeviceToHost));
+  if (hbad & 1) fail(SYMPROP_ERR_INVALID, "index out of range [1, %u]", t.dim);
+  if (hbad & 2) fail(SYMPROP_ERR_INVALID, "index tuple not sorted ascending");
+  raw.release();
+
+  // owners per tuple + ||X||^2 terms
+  DBuf<uint32_t> cnt(nnz + 1), off(nnz + 1);
+  DBuf<double> normsq(nnz + 1);
+  if (nnz) {
+    count_kernel<<<grid_for(nnz, 256), 256, 0, st>>>(t.inds.p, t.vals.p, nnz, N, cnt.p, normsq.p);
+    SPB_LAUNCH_CHECK();
+  }
+  SPB_CUDA(cudaMemset(cnt.p + nnz, 0, sizeof(uint32_t)));
+  DBuf<double> dsum(1);
+  {
+    size_t tmp = 0;
+    SPB_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp, cnt.p, off.p, nnz + 1, st));
+    size_t tmp2 = 0;
+    SPB_CUDA(cub::DeviceReduce::Sum(nullptr, tmp2, normsq.p, dsum.p, nnz, st));
+    DBuf<char> work(std::max<size_t>(std::max(tmp, tmp2), 1));
+    SPB_CUDA(cub::DeviceScan::ExclusiveSum(work.p, tmp, cnt.p, off.p, nnz + 1, st));
+    if (nnz) {
+      SPB_CUDA(cub::DeviceReduce::Sum(work.p, tmp2, normsq.p, dsum.p, nnz, st));
+    } else {
+      SPB_CUDA(cudaMemset(dsum.p, 0, sizeof(double)));
+    }
+  }
+  uint32_t total = 0;
+  double nsq = 0.0;
+  SPB_CUDA(cudaMemcpy(&total, off.p + nnz, sizeof(uint32_t), cudaMemcpyDeviceToHost));
+  SPB_CUDA(cudaMemcpy(&nsq, dsum.p, sizeof(double), cudaMemcpyDeviceToHost));
+  t.norm = std::sqrt(nsq);
+  t.nown = total;
+  t.sstride = ((N - 1) + 3) / 4 * 4;
+  if (N - 1 == 0) t.sstride = 4;
+
+  DBuf<uint32_t> own_row(t.nown), S_tmp(t.nown * t.sstride);
+  DBuf<double> c_tmp(t.nown);
+  if (nnz) {
+    emit_owners_kernel<<<grid_for(nnz, 128), 128, 0, st>>>(t.inds.p, t.vals.p, nnz, N, off.p,
+                                                           t.sstride, own_row.p, S_tmp.p,
+                                                           c_tmp.p);
+    SPB_LAUNCH_CHECK();
+  }
+  cnt.release();
+  off.release();
+  normsq.release();
+
+  // stable radix sort of owners by row
+  DBuf<uint32_t> rows_sorted(t.nown), perm_in(t.nown), perm(t.nown);
+  if (t.nown) {
+    std::vector<uint32_t> iota(t.nown);
+    std::iota(iota.begin(), iota.end(), 0u);
+    SPB_CUDA(cudaMemcpy(perm_in.p, iota.data(), t.nown * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    int end_bit = bits_for(t.dim);
+    size_t tmp = 0;
+    SPB_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, own_row.p, rows_sorted.p, perm_in.p,
+                                             perm.p, t.nown, 0, end_bit, st));
+    DBuf<char> work(std::max<size_t>(tmp, 1));
+    SPB_CUDA(cub::DeviceRadixSort::SortPairs(work.p, tmp, own_row.p, rows_sorted.p, perm_in.p,
+                                             perm.p, t.nown, 0, end_bit, st));
+  }
+  t.own_S.alloc(t.nown * t.sstride);
+  t.own_c64.alloc(t.nown);
+  t.own_c32.alloc(t.nown);
+  if (t.nown) {
+    gather_owners_kernel<<<grid_for(t.nown, 256), 256, 0, st>>>(perm.p, t.nown, t.sstride, S_tmp.p,
+                                                                c_tmp.p, t.own_S.p, t.own_c64.p,
+                                                                t.own_c32.p);
+    SPB_LAUNCH_CHECK();
+  }
+  t.row_ptr.alloc((uint64_t)t.dim + 1);
+  row_ptr_kernel<<<grid_for((uint64_t)t.dim + 1, 256), 256, 0, st>>>(rows_sorted.p, t.nown, t.dim,
+                                                                     t.row_ptr.p);
+  SPB_LAUNCH_CHECK();
+  t.h_row_ptr.resize((size_t)t.dim + 1);
+  SPB_CUDA(cudaMemcpy(t.h_row_ptr.data(), t.row_ptr.p, ((size_t)t.dim + 1) * sizeof(uint64_t),
+                      cudaMemcpyDeviceToHost));
+
+  // Work items: rows with more than chunk_owners owners are cut into slices
+  // whose partial sums a second kernel adds in a fixed order.
+  const uint64_t target_items = 148ull * 8ull;
+  uint64_t co = (t.nown + target_items - 1) / std::max<uint64_t>(target_items, 1);
+  co = std::min<uint64_t>(std::max<uint64_t>(co, 16), 256);
+  t.chunk_owners = (uint32_t)co;
+  std::vector<Chunk> ch;
+  std::vector<SplitRow> sp;
+  ch.reserve((size_t)t.dim + t.nown / co + 1);
+  uint32_t slot = 0;
+  for (uint32_t i = 0; i < t.dim; ++i) {
+    uint64_t b = t.h_row_ptr[i], e = t.h_row_ptr[(size_t)i + 1];
+    uint64_t c = e - b;
+    if (c <= co) {
+      ch.push_back(Chunk{i, kDirect, b, e});
+    } else {
+      uint32_t s0 = slot;
+      for (uint64_t x = b; x < e; x += co) ch.push_back(Chunk{i, slot++, x, std::min(e, x + co)});
+      sp.push_back(SplitRow{i, s0, slot, 0});
+    }
+  }
+  std::stable_sort(ch.begin(), ch.end(), [](const Chunk &a, const Chunk &b) {
+    return (a.oe - a.ob) > (b.oe - b.ob);
+  });
+  t.nchunks = (uint32_t)ch.size();
+  t.nsplit = (uint32_t)sp.size();
+  t.nslots = slot;
+  t.chunks.alloc(ch.size());
+  if (!ch.empty())
+    SPB_CUDA(cudaMemcpy(t.chunks.p, ch.data(), ch.size() * sizeof(Chunk), cudaMemcpyHostToDevice));
+  t.split.alloc(sp.size());
+  if (!sp.empty())
+    SPB_CUDA(cudaMemcpy(t.split.p, sp.data(), sp.size() * sizeof(SplitRow), cudaMemcpyHostToDevice));
+  SPB_CUDA(cudaDeviceSynchronize());
+}
+
+}  // namespace spb

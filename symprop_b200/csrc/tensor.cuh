@@ -1,0 +1,107 @@
+// Device-resident sparse symmetric tensor and the structures the S3TTMc
+// kernels consume.
+//
+// Layout in HBM (all row-major, 0-based ids):
+//   inds      nnz x order uint32         sorted unique tuples
+//   vals      nnz double
+//   own_S     nown x sstride uint32      the N-1 ids of each owner's leaf
+//                                        (sub-multiset t \ t_j), padded to a
+//                                        multiple of 4 ids (16-byte rows)
+//   own_c64   nown double                owner coefficient f_j * v*mult(t)/N!
+//   own_c32   nown float                 (FP32 copy)
+//   row_ptr   dim+1 uint64               owners of row i: [row_ptr[i], row_ptr[i+1])
+//   chunks    nchunks Chunk              work items: one row or a slice of a
+//                                        long row; heaviest first
+//   split     nsplit SplitRow            rows cut into several chunks and the
+//                                        partial-sum slots that hold them
+//
+// Owners are the reference's (leaf, rem, value) records
+// (src/compressed_dtree.cpp:67-74) re-segmented by their remaining index, so
+// every Y row is produced by one reduction and no Y element needs a global
+// atomic.  Repeated ids inside a tuple give identical owners
+// (src/dtree.cpp:62-80 keeps them as duplicates); they are merged here with
+// their multiplicity f_j folded into the coefficient.
+#pragma once
+
+#include <map>
+#include <memory>
+
+#include "common.cuh"
+
+namespace spb {
+
+struct Chunk {
+  uint32_t row;
+  uint32_t slot;  // partial-sum slot, or kDirect when the chunk owns its row
+  uint64_t ob, oe;
+};
+static constexpr uint32_t kDirect = 0xffffffffu;
+
+struct SplitRow {
+  uint32_t row;
+  uint32_t slot_begin, slot_end;
+  uint32_t pad;
+};
+
+// Reference CompressedDTree arrays, built on demand (tree.cu).
+struct TreeLevels {
+  uint32_t depth = 0;
+  std::vector<uint64_t> size;                 // per level
+  std::vector<DBuf<uint32_t>> level_idx;      // per level
+  std::vector<DBuf<uint64_t>> level_ptr;      // per level (last: owner CSR)
+  std::vector<DBuf<uint64_t>> dep_list;       // per level (l >= 1)
+  uint64_t nown = 0;
+  DBuf<uint64_t> own_rem;
+  DBuf<double> own_val;
+};
+
+// Per-(order, R) index tables for the packed recursion (s3ttmc.cu).
+struct PackedTables;
+
+struct TensorState {
+  int device = 0;
+  uint32_t order = 0, dim = 0;
+  uint64_t nnz = 0;
+  double norm = 0.0;
+
+  DBuf<uint32_t> inds;
+  DBuf<double> vals;
+
+  uint64_t nown = 0;
+  uint32_t sstride = 0;
+  DBuf<uint32_t> own_S;
+  DBuf<double> own_c64;
+  DBuf<float> own_c32;
+  DBuf<uint64_t> row_ptr;
+  std::vector<uint64_t> h_row_ptr;
+
+  uint32_t chunk_owners = 0;  // max owners per chunk
+  uint32_t nchunks = 0;
+  DBuf<Chunk> chunks;
+  uint32_t nsplit = 0, nslots = 0;
+  DBuf<SplitRow> split;
+
+  DBuf<double> partials;  // nslots x m partial sums (grown on demand)
+  DBuf<char> scratch;     // packed staging for unpacked output (grown on demand)
+  DBuf<char> io_U, io_Y;  // device staging of the host-pointer entry point
+
+  std::map<uint32_t, std::shared_ptr<PackedTables>> tables;  // by R
+  std::unique_ptr<TreeLevels> tree;
+};
+
+// s3ttmc.cu
+void s3ttmc_run(TensorState &t, const void *dU, uint32_t R, bool packed, void *dY,
+                int precision, cudaStream_t stream);
+uint32_t s3ttmc_launch_count(const TensorState &t, uint32_t R, bool packed);
+void unpack_rows(const void *dpacked, uint64_t rows, uint32_t dim, uint32_t order,
+                 void *dfull, int precision, cudaStream_t stream);
+// tree.cu
+void tree_build(TensorState &t);
+// tensor.cu
+void tensor_build(TensorState &t, const uint32_t *h_inds, const double *h_vals);
+
+}  // namespace spb
+
+struct symprop_tensor {
+  spb::TensorState s;
+};

@@ -1,0 +1,56 @@
+"""CPU tests of the drop-in boundary: the C-ABI library loads and exports
+every entry point declared in include/symprop.h; host-only helpers work
+without a GPU (no compute call is made here)."""
+import ctypes
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+import symprop_b200 as sp
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    text = open(os.path.join(ROOT, "include", "symprop.h")).read()
+    return sorted(set(re.findall(r"\b(symprop_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    L = sp.lib()
+    names = declared_symbols()
+    assert len(names) >= 20
+    missing = [n for n in names if not hasattr(L, n)]
+    assert not missing, missing
+    assert set(sp.exported_symbols()) <= set(names)
+
+
+def test_status_strings_and_host_helpers():
+    L = sp.lib()
+    assert L.symprop_status_string(0) == b"ok"
+    assert L.symprop_status_string(2) == b"unsupported order"
+    assert sp.symtens_size(16, 3) == 816
+    c = sp.symtens_coeff(3, 3)
+    assert c.sum() == 27
+
+
+def test_headers_compile_as_c_and_cpp(tmp_path):
+    src = tmp_path / "t.c"
+    src.write_text('#include "symprop.h"\nint main(void){return SYMPROP_OK;}\n')
+    subprocess.run(["gcc", "-std=c99", "-I", os.path.join(ROOT, "include"), "-c", str(src), "-o",
+                    str(tmp_path / "t.o")], check=True)
+    cpp = tmp_path / "t.cpp"
+    cpp.write_text('#include "symtucker.hpp"\nint main(){symprop::Config c; return (int)c.rank - 2;}\n')
+    subprocess.run(["/usr/bin/g++", "-std=c++20", "-I", os.path.join(ROOT, "include"), "-c",
+                    str(cpp), "-o", str(tmp_path / "t2.o")], check=True)
+
+
+def test_cli_help_and_unknown_flag():
+    cli = sp.CLI_PATH
+    r = subprocess.run([cli, "-h"], capture_output=True, text=True)
+    assert r.returncode == 1 and "-f <input_file>" in r.stdout
+    r = subprocess.run([cli, "-zz"], capture_output=True, text=True)
+    assert r.returncode == 1 and "Option -zz is not defined" in r.stdout
