@@ -109,6 +109,11 @@ int symprop_s3ttmc(const symprop_tensor *t, const void *U, uint32_t R,
 /* Same with device pointers on `stream`; Y is written asynchronously. */
 int symprop_s3ttmc_device(const symprop_tensor *t, const void *dU, uint32_t R,
                           int packed, void *dY, int precision, void *stream);
+/* Selects the S3TTMc schedule for the whole process: 0 automatic (default:
+ * register-tiled where the shape is supported), 1 per-owner rows kernel,
+ * 2 register-tiled only.  Both compute the same Y; tests use this to check
+ * each schedule against the oracle. */
+int symprop_s3ttmc_schedule(int schedule);
 /* Number of kernel launches one symprop_s3ttmc_device call issues for
  * (R, packed); lets callers count their launches. */
 int symprop_s3ttmc_launches(const symprop_tensor *t, uint32_t R, int packed,
@@ -124,6 +129,17 @@ int symprop_symtens_coeff(uint32_t dim, uint32_t order, double *coeff);
 int symprop_unpack_rows_device(const double *dpacked, uint64_t rows,
                                uint32_t dim, uint32_t order, double *dfull,
                                void *stream);
+
+/* ---------------------------------------------------------- dense step */
+/* Packed Gram matrix G = (Y diag(scale))^T (Y diag(scale)) (m x m, FP64,
+ * full symmetric) of a device n x m row-major Y, the dense step HOOI uses
+ * in place of leftsvd(Y) (src/sparse/spsymtensor.cpp:225,
+ * src/dense/matrixops.cpp:18-43; symsyrk :126-146 is its n x n twin).
+ * precision SYMPROP_FP64: dY, dscale are double*, FP64 CUDA-core GEMM;
+ * SYMPROP_FP32: dY, dscale are float*, tcgen05 tensor cores with split-BF16
+ * operands and FP32 accumulation. */
+int symprop_gram_device(const void *dY, uint64_t n, uint32_t m, const void *dscale,
+                        double *dG, int precision, void *stream);
 
 /* ------------------------------------------------------------- Tucker */
 typedef struct {

@@ -92,6 +92,8 @@ def lib():
         "symprop_unpack_rows_device": (_I, [_P, _U64, _U32, _U32, _P, _P]),
         "symprop_tucker": (_I, [_P, ctypes.POINTER(Config), _I, ctypes.POINTER(_Result)]),
         "symprop_write_decomp": (_I, [ctypes.c_char_p, _P, _P, _U32, _U32, _U32, _I]),
+        "symprop_gram_device": (_I, [_P, _U64, _U32, _P, _P, _I, _P]),
+        "symprop_s3ttmc_schedule": (_I, [_I]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -109,7 +111,7 @@ def exported_symbols() -> list[str]:
         "symprop_tree_level_size", "symprop_tree_owner_count", "symprop_tree_copy_level",
         "symprop_tree_copy_owners", "symprop_s3ttmc", "symprop_s3ttmc_device", "symprop_s3ttmc_launches",
         "symprop_symtens_size", "symprop_symtens_coeff", "symprop_unpack_rows_device", "symprop_tucker",
-        "symprop_write_decomp",
+        "symprop_write_decomp", "symprop_gram_device", "symprop_s3ttmc_schedule",
     ]
 
 
@@ -127,6 +129,13 @@ def device_count() -> int:
     n = _I(0)
     _check(lib().symprop_device_count(ctypes.byref(n)))
     return n.value
+
+
+def gram_device(dY_ptr: int, n: int, m: int, dscale_ptr: int, dG_ptr: int, precision: int = FP64,
+                stream: int = 0) -> None:
+    """G = (Y diag(scale))^T (Y diag(scale)) on the device (FP64 CUDA cores or
+    FP32 input on tcgen05 tensor cores with split-BF16 operands)."""
+    _check(lib().symprop_gram_device(_P(dY_ptr), n, m, _P(dscale_ptr), _P(dG_ptr), precision, _P(stream)))
 
 
 def symtens_size(dim: int, order: int) -> int:
@@ -228,6 +237,16 @@ class SpSymtensor:
         return v.value
 
     # ---- CompressedDTree export (src/compressed_dtree.cpp:13-131)
+    def tree_level_sizes(self) -> list:
+        L = lib()
+        _check(L.symprop_tree_build(self._h))
+        out = []
+        for l in range(self._order - 1):
+            sz = _U64(0)
+            _check(L.symprop_tree_level_size(self._h, l, ctypes.byref(sz)))
+            out.append(sz.value)
+        return out
+
     def tree(self) -> dict:
         L = lib()
         _check(L.symprop_tree_build(self._h))

@@ -6,6 +6,8 @@
 #include <iostream>
 #include <mutex>
 
+#include "dense.cuh"
+#include "gram_tc.cuh"
 #include "tensor.cuh"
 
 namespace spb {
@@ -197,10 +199,45 @@ int symprop_s3ttmc(const symprop_tensor *t, const void *U, uint32_t R, int packe
   });
 }
 
+int symprop_s3ttmc_schedule(int schedule) {
+  return guard([&] {
+    require(schedule >= 0 && schedule <= 2, "schedule must be 0, 1 or 2");
+    set_s3ttmc_schedule(schedule);
+  });
+}
+
 int symprop_s3ttmc_launches(const symprop_tensor *t, uint32_t R, int packed, uint32_t *launches) {
   return guard([&] {
     require(t && launches, "null argument");
     *launches = s3ttmc_launch_count(t->s, R, packed != 0);
+  });
+}
+
+int symprop_gram_device(const void *dY, uint64_t n, uint32_t m, const void *dscale, double *dG,
+                        int precision, void *stream) {
+  return guard([&] {
+    require(dY && dscale && dG, "null argument");
+    require(n > 0 && m > 0 && n < (1ull << 31), "bad sizes");
+    cudaStream_t st = (cudaStream_t)stream;
+    if (precision == SYMPROP_FP64) {
+      const double *Y = (const double *)dY, *sd = (const double *)dscale;
+      dense::gemm<double>(st, (int)m, (int)m, (int)n, 1.0, Y, (int)m, true, Y, (int)m, false, 0.0, dG,
+                          (int)m, nullptr, true);
+      dense::scale_sym(st, dG, (int)m, sd);
+    } else if (precision == SYMPROP_FP32) {
+      DBuf<char> ws(gram::workspace_bytes((int)n, (int)m));
+      DBuf<int> err(1);
+      SPB_CUDA(cudaMemsetAsync(err.p, 0, sizeof(int), st));
+      gram::gram_split_bf16(st, (const float *)dY, (int)n, (int)m, (const float *)dscale, dG, ws.p,
+                            err.p);
+      int h = 0;
+      SPB_CUDA(cudaMemcpyAsync(&h, err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+      SPB_CUDA(cudaStreamSynchronize(st));
+      if (h) fail(SYMPROP_ERR_TIMEOUT, "tensor-core Gram: a bounded wait expired");
+    } else {
+      fail(SYMPROP_ERR_INVALID, "unknown precision");
+    }
+    SPB_CUDA(cudaStreamSynchronize(st));
   });
 }
 

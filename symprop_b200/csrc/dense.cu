@@ -393,6 +393,13 @@ __global__ void __launch_bounds__(1024) jacobi_kernel(const double *S, int n, do
 
 // ------------------------------------------------------------- misc
 
+__global__ void scale_sym_kernel(double *G, int m, const double *sd) {
+  size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (size_t)m * m) return;
+  int i = (int)(idx / m), j = (int)(idx % m);
+  G[idx] *= sd[i] * sd[j];
+}
+
 __global__ void clip_rows_kernel(double *U, int n, int r, double delta) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -569,6 +576,11 @@ void jacobi_eig(cudaStream_t st, const double *S, int n, double *w, double *V) {
   size_t smem = 2 * sizeof(double) * np * np;
   SPB_CUDA(cudaFuncSetAttribute(jacobi_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   jacobi_kernel<<<1, 1024, smem, st>>>(S, n, w, V);
+  SPB_LAUNCH_CHECK();
+}
+
+void scale_sym(cudaStream_t st, double *G, int m, const double *sd) {
+  scale_sym_kernel<<<cdiv((long long)m * m, 256), 256, 0, st>>>(G, m, sd);
   SPB_LAUNCH_CHECK();
 }
 

@@ -45,6 +45,7 @@ int top_eigs(cudaStream_t st, const double *S, int s, int r, double *V, double *
              const double *warm, double tol, int max_restarts);
 
 // elementwise helpers
+void scale_sym(cudaStream_t st, double *G, int m, const double *sd);  // G[i][j] *= sd[i] sd[j]
 void scale_rows_clip(cudaStream_t st, double *U, int n, int r, double delta);
 template <typename Ts, typename Td> void convert(cudaStream_t st, const Ts *src, Td *dst, size_t n);
 

@@ -18,11 +18,16 @@
 //  * FP32 mode accumulates each owner's contribution in FP32 and folds
 //    batches into a Kahan-compensated accumulator.
 #include <algorithm>
+#include <atomic>
 #include <cstdlib>
 
+#include "s3ttmc_tiled.cuh"
 #include "tensor.cuh"
 
 namespace spb {
+
+static void finish_rows(TensorState &t, uint64_t m, void *Ypk, bool packed, void *dY, uint32_t R,
+                        uint32_t L, int precision, cudaStream_t st);
 
 static constexpr int kMaxL = 7;          // orders 2..8
 static constexpr uint32_t kURow = 0x80000000u;
@@ -445,13 +450,25 @@ void s3ttmc_run(TensorState &t, const void *dU, uint32_t R, bool packed, void *d
     SPB_CUDA(cudaMemsetAsync(dY, 0, (size_t)t.dim * ldy * es, st));
     return;
   }
-  PackedTables &tb = tables_for(t, R);
   void *Ypk = dY;
   if (!packed) {
     t.scratch.ensure((size_t)t.dim * m * es);
     Ypk = t.scratch.p;
   }
   if (t.nslots) t.partials.ensure((size_t)t.nslots * m);
+  const int sched = s3ttmc_schedule();
+  if (sched != kScheduleRows) {
+    auto it = t.tiled.find(R);
+    if (it == t.tiled.end()) it = t.tiled.emplace(R, tiled_plan(t.order, R)).first;
+    if (tiled_supported(*it->second)) {
+      tiled_launch(*it->second, t, dU, Ypk, precision, st);
+      finish_rows(t, m, Ypk, packed, dY, R, L, precision, st);
+      return;
+    }
+    if (sched == kScheduleTiled)
+      fail(SYMPROP_ERR_SIZE, "tiled S3TTMc does not support order %u rank %u", t.order, R);
+  }
+  PackedTables &tb = tables_for(t, R);
 
   RowParams rp{};
   rp.chunks = t.chunks.p;
@@ -485,6 +502,12 @@ void s3ttmc_run(TensorState &t, const void *dU, uint32_t R, bool packed, void *d
     else
       dispatch_rows<float>(L, tb, rp, t.nchunks, smem, st);
   }
+  finish_rows(t, m, Ypk, packed, dY, R, L, precision, st);
+}
+
+// combine the partial rows of split rows; unpack if requested
+static void finish_rows(TensorState &t, uint64_t m, void *Ypk, bool packed, void *dY, uint32_t R,
+                        uint32_t L, int precision, cudaStream_t st) {
   if (t.nsplit) {
     if (precision == SYMPROP_FP64)
       combine_kernel<double><<<t.nsplit, 256, 0, st>>>(t.split.p, t.partials.p, (uint32_t)m, Ypk, m);
@@ -494,5 +517,9 @@ void s3ttmc_run(TensorState &t, const void *dU, uint32_t R, bool packed, void *d
   }
   if (!packed) unpack_rows(Ypk, t.dim, R, L, dY, precision, st);
 }
+
+static std::atomic<int> g_schedule{kScheduleAuto};
+int s3ttmc_schedule() { return g_schedule.load(); }
+void set_s3ttmc_schedule(int s) { g_schedule.store(s); }
 
 }  // namespace spb

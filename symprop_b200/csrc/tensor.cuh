@@ -53,10 +53,19 @@ struct TreeLevels {
   uint64_t nown = 0;
   DBuf<uint64_t> own_rem;
   DBuf<double> own_val;
+  DBuf<double> leaf_mult;  // distinct orderings of each leaf multiset
 };
 
-// Per-(order, R) index tables for the packed recursion (s3ttmc.cu).
+// Per-(order, R) index tables for the packed recursion (s3ttmc.cu) and the
+// register-tiled schedule (s3ttmc_tiled.cu).
 struct PackedTables;
+struct TiledPlan;
+
+// S3TTMc schedule: 0 = automatic (tiled where supported), 1 = per-owner
+// rows kernel, 2 = tiled (error if unsupported).
+enum { kScheduleAuto = 0, kScheduleRows = 1, kScheduleTiled = 2 };
+int s3ttmc_schedule();
+void set_s3ttmc_schedule(int s);
 
 struct TensorState {
   int device = 0;
@@ -86,6 +95,7 @@ struct TensorState {
   DBuf<char> io_U, io_Y;  // device staging of the host-pointer entry point
 
   std::map<uint32_t, std::shared_ptr<PackedTables>> tables;  // by R
+  std::map<uint32_t, std::shared_ptr<TiledPlan>> tiled;      // by R
   std::unique_ptr<TreeLevels> tree;
 };
 

@@ -112,6 +112,25 @@ __global__ void last_id_kernel(const uint64_t *nodes, uint64_t n, KeyFmt f, uint
   if (j < n) idx[j] = key_elem(nodes + j * f.words, f.len - 1, f.b, f.E);
 }
 
+// (N-1)! / prod(freq!) of each leaf multiset
+__global__ void leaf_mult_kernel(const uint64_t *nodes, uint64_t n, KeyFmt f, double *out) {
+  uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  uint64_t denom = 1, run = 1;
+  uint32_t prev = key_elem(nodes + j * f.words, 0, f.b, f.E);
+  for (int i = 1; i <= f.len; ++i) {
+    uint32_t x = i < f.len ? key_elem(nodes + j * f.words, i, f.b, f.E) : 0xffffffffu;
+    if (i < f.len && x == prev) {
+      ++run;
+    } else {
+      denom *= factorial_u64((int)run);
+      run = 1;
+    }
+    prev = x;
+  }
+  out[j] = (double)(factorial_u64(f.len) / denom);
+}
+
 __device__ int cmp_key(const uint64_t *a, const uint64_t *b, int nw) {
   for (int w = 0; w < nw; ++w)
     if (a[w] != b[w]) return a[w] < b[w] ? -1 : 1;
@@ -273,6 +292,11 @@ void tree_build(TensorState &t) {
       if (cnt) {
         owners_kernel<<<grid(cnt), 256, 0, st>>>(perm.p, cnt, t.inds.p, t.vals.p, N, tr->own_rem.p,
                                                  tr->own_val.p);
+        SPB_LAUNCH_CHECK();
+      }
+      tr->leaf_mult.alloc(std::max<uint64_t>(nu, 1));
+      if (nu) {
+        leaf_mult_kernel<<<grid(nu), 256, 0, st>>>(nodes[l].p, nu, f, tr->leaf_mult.p);
         SPB_LAUNCH_CHECK();
       }
     } else {

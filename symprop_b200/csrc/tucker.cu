@@ -1,6 +1,389 @@
-// placeholder, replaced by the Tucker drivers
+// Tucker drivers on the GPU: HOOI, HOQRI and AltHOOI with the reference's
+// control flow, stopping rule and printed lines.
+//
+//   TuckerHOOI    src/sparse/spsymtensor.cpp:201-252
+//   TuckerHOQRI   src/sparse/spsymtensor.cpp:254-299
+//   TuckerAltHOOI src/sparse/spsymtensor.cpp:301-337
+//   regularize    src/sparse/spsymtensor.cpp:168-199
+//   random init   src/tucker.cpp:25-36 (std::mt19937(seed) +
+//                 std::normal_distribution<double>(0,1), row-major dim x rank)
+//   hosvd_init    src/sparse/spsymtensor.cpp:339-383
+//   error         src/tucker.cpp:40-45: sqrt(||X||^2 - ||C||^2) / ||X||
+//
+// HOOI's leftsvd of the unpacked n x R^(N-1) Y is replaced by the packed
+// Gram: Y_unp Y_unp^T = Y D Y^T with D the permutation counts of the packed
+// columns (every packed column appears D_q times in the unpacked Y), so the
+// leading left singular subspace is the top-r eigenspace of Y D Y^T
+// (n <= m) or U = orth(Y D^1/2 V) with V the top-r eigenvectors of
+// D^1/2 Y^T Y D^1/2 (n > m).  ||C||^2 of the unpacked core is the
+// D-weighted norm of the packed core U^T Y.  Every later step is invariant
+// under U -> U Q for orthogonal Q, so the error trajectory does not depend on
+// which orthonormal basis LAPACK or this code returns; the printed "relative
+// residual" compares cores in those bases and is basis-dependent.
+#include <chrono>
+#include <cmath>
+#include <iomanip>
+#include <iostream>
+#include <random>
+#include <vector>
+
+#include "dense.cuh"
+#include "gram_tc.cuh"
 #include "tensor.cuh"
-extern "C" int symprop_tucker(const symprop_tensor *, const symprop_config *, int, symprop_result *) {
-  spb::set_last_error("not built yet");
-  return SYMPROP_ERR_INVALID;
+
+namespace spb {
+namespace {
+
+__global__ void scale_sym_kernel(double *G, int m, const double *sd) {
+  size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (size_t)m * m) return;
+  int i = (int)(idx / m), j = (int)(idx % m);
+  G[idx] *= sd[i] * sd[j];
+}
+
+// A += mult(C) w_C w_C^T over the leaves C of the tree (hoevd init):
+// A = X_(1) X_(1)^T (src/sparse/spsymtensor.cpp:385-439).
+__global__ void hoevd_syrk_kernel(const uint64_t *own_ptr, const uint64_t *rem, const double *val,
+                                  const double *leaf_mult, uint64_t nleaf, int n, double *A) {
+  uint64_t leaf = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (leaf >= nleaf) return;
+  uint64_t b = own_ptr[leaf], e = own_ptr[leaf + 1];
+  double mult = leaf_mult[leaf];
+  for (uint64_t i = b; i < e; ++i) {
+    if (i > b && rem[i] == rem[i - 1]) continue;  // repeated ids give duplicate owners
+    for (uint64_t j = i; j < e; ++j) {
+      if (j > i && rem[j] == rem[j - 1]) continue;
+      uint64_t p = rem[i] - 1, q = rem[j] - 1;
+      double v = mult * val[i] * val[j];
+      atomicAdd(&A[p * n + q], v);
+      if (p != q) atomicAdd(&A[q * n + p], v);
+    }
+  }
+}
+
+struct Timer {
+  cudaEvent_t a, b;
+  cudaStream_t st;
+  explicit Timer(cudaStream_t s) : st(s) {
+    SPB_CUDA(cudaEventCreate(&a));
+    SPB_CUDA(cudaEventCreate(&b));
+  }
+  ~Timer() {
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+  }
+  void start() { SPB_CUDA(cudaEventRecord(a, st)); }
+  double stop_ms() {
+    SPB_CUDA(cudaEventRecord(b, st));
+    SPB_CUDA(cudaEventSynchronize(b));
+    float ms = 0;
+    SPB_CUDA(cudaEventElapsedTime(&ms, a, b));
+    return ms;
+  }
+};
+
+void regularize(cudaStream_t st, double *U, int n, int r, double delta) {
+  dense::scale_rows_clip(st, U, n, r, delta);
+  dense::orthonormalize(st, U, n, r);  // leftsvd(U) -> any orthonormal basis of its span
+}
+
+}  // namespace
+
+void hoevd_factor(TensorState &t, cudaStream_t st, int r, double *U, bool print_matrix);
+
+int run_tucker(TensorState &t, const symprop_config &c, int alg, symprop_result &res) {
+  const int n = (int)t.dim, N = (int)t.order, r = (int)c.rank;
+  if (r < 1) fail(SYMPROP_ERR_INVALID, "rank must be positive");
+  if (r > n) fail(SYMPROP_ERR_INVALID, "rank %d exceeds dim %d", r, n);
+  if (N < 3) fail(SYMPROP_ERR_ORDER, "Tucker needs order >= 3");
+  if (alg < 0 || alg > 2) fail(SYMPROP_ERR_INVALID, "unknown algorithm %d", alg);
+  const bool mixed = c.precision == SYMPROP_PREC_MIXED;
+  const int L = N - 1;
+  const uint64_t m64 = symsize(r, L);
+  if (m64 > (1u << 30)) fail(SYMPROP_ERR_SIZE, "packed width too large");
+  const int m = (int)m64;
+  uint64_t full = 1;
+  for (int j = 0; j < L; ++j) full *= (uint64_t)r;
+  const double normX = t.norm;
+
+  cudaStream_t st;
+  SPB_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+  struct StreamGuard {
+    cudaStream_t s;
+    ~StreamGuard() { cudaStreamDestroy(s); }
+  } sg{st};
+  Timer tall(st), tphase(st);
+  auto wall0 = std::chrono::steady_clock::now();
+  tall.start();
+
+  // packed-column weights D (src/dense/symtensor.cpp:53-59)
+  std::vector<double> hD(m), hsD(m);
+  for_each_sorted((uint32_t)r, L, [&](const std::vector<uint32_t> &q, uint64_t lin) {
+    uint64_t denom = 1, run = 1;
+    for (size_t j = 1; j <= q.size(); ++j) {
+      if (j < q.size() && q[j] == q[j - 1]) ++run;
+      else { denom *= factorial_u64((int)run); run = 1; }
+    }
+    hD[lin] = (double)(factorial_u64(L) / denom);
+    hsD[lin] = std::sqrt(hD[lin]);
+  });
+  DBuf<double> dD(m), dsD(m);
+  SPB_CUDA(cudaMemcpy(dD.p, hD.data(), sizeof(double) * m, cudaMemcpyHostToDevice));
+  SPB_CUDA(cudaMemcpy(dsD.p, hsD.data(), sizeof(double) * m, cudaMemcpyHostToDevice));
+
+  // factor initialisation
+  DBuf<double> U((size_t)n * r), Uprev((size_t)n * r);
+  {
+    std::vector<double> h((size_t)n * r);
+    std::normal_distribution<double> distr(0.0, 1.0);
+    std::mt19937 engine{(std::mt19937::result_type)c.seed};
+    for (size_t i = 0; i < h.size(); i++) h[i] = distr(engine);
+    if (c.init == SYMPROP_INIT_USER) {
+      if (!res.init_factor) fail(SYMPROP_ERR_INVALID, "init_factor is null");
+      std::copy(res.init_factor, res.init_factor + h.size(), h.begin());
+    }
+    SPB_CUDA(cudaMemcpy(U.p, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice));
+    // AltHOOI keeps the factor before hosvd_init as factor_prev (spsymtensor.cpp:306-308)
+    SPB_CUDA(cudaMemcpy(Uprev.p, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice));
+  }
+  if (c.init == SYMPROP_INIT_HOSVD) {
+    // non-MKL reference build: prints and leaves the random factor
+    // (src/sparse/matrixops.cpp:15-17)
+    std::printf("Error: sparse SVD requires MKL.\n");
+    std::fflush(stdout);
+  } else if (c.init == SYMPROP_INIT_HOEVD) {
+    hoevd_factor(t, st, r, U.p, c.verbose != 0);
+  }
+
+  const bool gram_nn = n <= m;  // n x n form (AltHOOI's symsyrk) vs m x m Gram
+  const int s = gram_nn ? n : m;
+  DBuf<double> Y((size_t)n * m);
+  DBuf<float> Y32(mixed ? (size_t)n * m : 0), U32(mixed ? (size_t)n * r : 0);
+  DBuf<float> S32(mixed ? (size_t)s * s : 0), V32(mixed ? (size_t)s * r : 0),
+      core32(mixed ? (size_t)r * m : 0), W32(mixed ? (size_t)n * r : 0), sD32(mixed ? m : 0),
+      D32(mixed ? m : 0);
+  if (mixed) {
+    dense::convert<double, float>(st, dsD.p, sD32.p, m);
+    dense::convert<double, float>(st, dD.p, D32.p, m);
+  }
+  DBuf<char> gram_ws(mixed && !gram_nn ? gram::workspace_bytes(n, m) : 0);
+  DBuf<int> gram_err(1);
+  SPB_CUDA(cudaMemsetAsync(gram_err.p, 0, sizeof(int), st));
+  DBuf<double> S((size_t)s * s), V((size_t)s * r), Vwarm((size_t)s * r);
+  DBuf<double> core((size_t)r * m), core_prev((size_t)r * m), red(2);
+  SPB_CUDA(cudaMemsetAsync(core_prev.p, 0, sizeof(double) * r * m, st));
+  bool have_warm = false;
+  std::vector<double> lam(r);
+  const double eig_tol = mixed ? 1e-7 : 1e-12;
+
+  double prev_error = 0.0, error = 0.0, cn2 = 0.0;
+  double s3_ms = 0, dense_ms = 0;
+  uint64_t iters = 0;
+  int status = SYMPROP_OK;
+  const int prec_digits = alg == SYMPROP_ALTHOOI ? 10 : 12;
+
+  for (uint64_t iter = 0; iter < c.max_iter; ++iter) {
+    tphase.start();
+    regularize(st, U.p, n, r, c.delta);
+    dense_ms += tphase.stop_ms();
+
+    tphase.start();
+    if (mixed) {
+      dense::convert<double, float>(st, U.p, U32.p, (size_t)n * r);
+      s3ttmc_run(t, U32.p, (uint32_t)r, true, Y32.p, SYMPROP_FP32, st);
+    } else {
+      s3ttmc_run(t, U.p, (uint32_t)r, true, Y.p, SYMPROP_FP64, st);
+    }
+    s3_ms += tphase.stop_ms();
+
+    tphase.start();
+    double rel_res = 0.0;
+    if (alg == SYMPROP_HOOI || alg == SYMPROP_ALTHOOI) {
+      // leading r-dimensional left singular subspace of Y D^1/2
+      if (gram_nn) {
+        if (mixed) {
+          dense::gemm<float>(st, n, n, m, 1.f, Y32.p, m, false, Y32.p, m, true, 0.f, S32.p, n, D32.p, true);
+          dense::convert<float, double>(st, S32.p, S.p, (size_t)n * n);
+        } else {
+          dense::gemm<double>(st, n, n, m, 1.0, Y.p, m, false, Y.p, m, true, 0.0, S.p, n, dD.p, true);
+        }
+        int e = dense::top_eigs(st, S.p, n, r, V.p, lam.data(), have_warm ? Vwarm.p : nullptr,
+                                eig_tol, 60);
+        if (e != SYMPROP_OK) status = e;
+        SPB_CUDA(cudaMemcpyAsync(U.p, V.p, sizeof(double) * n * r, cudaMemcpyDeviceToDevice, st));
+      } else {
+        if (mixed) {
+          // tcgen05 split-BF16 Gram of Y D^1/2 (FP32 accumulation)
+          gram::gram_split_bf16(st, Y32.p, n, m, sD32.p, S.p, gram_ws.p, gram_err.p);
+        } else {
+          dense::gemm<double>(st, m, m, n, 1.0, Y.p, m, true, Y.p, m, false, 0.0, S.p, m, nullptr, true);
+          scale_sym_kernel<<<(unsigned)(((size_t)m * m + 255) / 256), 256, 0, st>>>(S.p, m, dsD.p);
+          SPB_LAUNCH_CHECK();
+        }
+        int e = dense::top_eigs(st, S.p, m, r, V.p, lam.data(), have_warm ? Vwarm.p : nullptr,
+                                eig_tol, 60);
+        if (e != SYMPROP_OK) status = e;
+        if (mixed) {
+          dense::convert<double, float>(st, V.p, V32.p, (size_t)m * r);
+          dense::gemm<float>(st, n, r, m, 1.f, Y32.p, m, false, V32.p, r, false, 0.f, W32.p, r, sD32.p);
+          dense::convert<float, double>(st, W32.p, U.p, (size_t)n * r);
+        } else {
+          dense::gemm<double>(st, n, r, m, 1.0, Y.p, m, false, V.p, r, false, 0.0, U.p, r, dsD.p);
+        }
+        dense::orthonormalize(st, U.p, n, r);
+      }
+      SPB_CUDA(cudaMemcpyAsync(Vwarm.p, V.p, sizeof(double) * (size_t)s * r, cudaMemcpyDeviceToDevice, st));
+      have_warm = true;
+      // core = U^T Y (r x m packed)
+      if (mixed) {
+        dense::convert<double, float>(st, U.p, U32.p, (size_t)n * r);
+        dense::gemm<float>(st, r, m, n, 1.f, U32.p, r, true, Y32.p, m, false, 0.f, core32.p, m);
+        dense::convert<float, double>(st, core32.p, core.p, (size_t)r * m);
+      } else {
+        dense::gemm<double>(st, r, m, n, 1.0, U.p, r, true, Y.p, m, false, 0.0, core.p, m);
+      }
+      double h[2];
+      if (alg == SYMPROP_HOOI) {
+        // rel_residual(core_prev, core) on the unpacked cores
+        dense::weighted_sq<double>(st, core_prev.p, core.p, dD.p, r, m, red.p);
+        SPB_CUDA(cudaMemcpyAsync(h, red.p, sizeof(h), cudaMemcpyDeviceToHost, st));
+        SPB_CUDA(cudaStreamSynchronize(st));
+        rel_res = h[0] / h[1];
+      } else {
+        // rel_residual(factor, factor_prev)
+        dense::weighted_sq<double>(st, U.p, Uprev.p, nullptr, n, r, red.p);
+        SPB_CUDA(cudaMemcpyAsync(h, red.p, sizeof(h), cudaMemcpyDeviceToHost, st));
+        SPB_CUDA(cudaStreamSynchronize(st));
+        rel_res = h[0] / h[1];
+      }
+      dense::weighted_sq<double>(st, core.p, nullptr, dD.p, r, m, red.p);
+      SPB_CUDA(cudaMemcpyAsync(h, red.p, sizeof(h), cudaMemcpyDeviceToHost, st));
+      SPB_CUDA(cudaStreamSynchronize(st));
+      cn2 = h[1];
+    } else {  // HOQRI
+      if (mixed) {
+        dense::convert<double, float>(st, U.p, U32.p, (size_t)n * r);
+        dense::gemm<float>(st, r, m, n, 1.f, U32.p, r, true, Y32.p, m, false, 0.f, core32.p, m);
+        dense::convert<float, double>(st, core32.p, core.p, (size_t)r * m);
+        // U = Y diag(D) core^T  (symgemm, src/dense/matrixops.cpp:102-124)
+        dense::gemm<float>(st, n, r, m, 1.f, Y32.p, m, false, core32.p, m, true, 0.f, W32.p, r, D32.p);
+        dense::convert<float, double>(st, W32.p, U.p, (size_t)n * r);
+      } else {
+        dense::gemm<double>(st, r, m, n, 1.0, U.p, r, true, Y.p, m, false, 0.0, core.p, m);
+        dense::gemm<double>(st, n, r, m, 1.0, Y.p, m, false, core.p, m, true, 0.0, U.p, r, dD.p);
+      }
+      dense::orthonormalize(st, U.p, n, r);  // qr (src/dense/matrixops.cpp:58-75)
+      double h[2];
+      dense::weighted_sq<double>(st, core.p, core_prev.p, dD.p, r, m, red.p);
+      SPB_CUDA(cudaMemcpyAsync(h, red.p, sizeof(h), cudaMemcpyDeviceToHost, st));
+      SPB_CUDA(cudaStreamSynchronize(st));
+      rel_res = h[0] / h[1];  // symtens_rel_res (src/dense/symtensor.cpp:78-95)
+      cn2 = h[1];
+    }
+    dense_ms += tphase.stop_ms();
+    if (mixed && !gram_nn) {
+      int herr = 0;
+      SPB_CUDA(cudaMemcpy(&herr, gram_err.p, sizeof(int), cudaMemcpyDeviceToHost));
+      if (herr) fail(SYMPROP_ERR_TIMEOUT, "tensor-core Gram: a bounded wait expired");
+    }
+
+    error = std::sqrt(normX * normX - cn2) / normX;
+    if (iter < res.trace_cap) {
+      if (res.error_trace) res.error_trace[iter] = error;
+      if (res.relres_trace) res.relres_trace[iter] = rel_res;
+    }
+    if (c.verbose) {
+      std::cout << std::scientific << std::setprecision(prec_digits) << "Iteration: " << iter
+                << " relative residual: " << rel_res << " error " << error << "\n";
+    }
+    iters = iter + 1;
+    if (alg == SYMPROP_HOQRI) {
+      SPB_CUDA(cudaMemcpyAsync(core_prev.p, core.p, sizeof(double) * r * m, cudaMemcpyDeviceToDevice, st));
+    }
+    double error_diff = std::abs(prev_error - error);
+    if (error_diff < c.rel_tol) break;
+    prev_error = error;
+    if (alg == SYMPROP_HOOI) {
+      SPB_CUDA(cudaMemcpyAsync(core_prev.p, core.p, sizeof(double) * r * m, cudaMemcpyDeviceToDevice, st));
+    } else if (alg == SYMPROP_ALTHOOI) {
+      SPB_CUDA(cudaMemcpyAsync(Uprev.p, U.p, sizeof(double) * n * r, cudaMemcpyDeviceToDevice, st));
+    }
+  }
+
+  // outputs
+  const size_t csize = (size_t)r * full;
+  if (res.core) {
+    std::vector<double> hc(csize, 0.0);
+    if (alg == SYMPROP_ALTHOOI) {
+      // AltHOOI writes the packed r x m core into the front of _core
+      SPB_CUDA(cudaMemcpyAsync(hc.data(), core.p, sizeof(double) * r * m, cudaMemcpyDeviceToHost, st));
+    } else {
+      DBuf<double> cu(csize);
+      unpack_rows(core.p, (uint64_t)r, (uint32_t)r, (uint32_t)L, cu.p, SYMPROP_FP64, st);
+      SPB_CUDA(cudaMemcpyAsync(hc.data(), cu.p, sizeof(double) * csize, cudaMemcpyDeviceToHost, st));
+      SPB_CUDA(cudaStreamSynchronize(st));
+    }
+    SPB_CUDA(cudaStreamSynchronize(st));
+    std::copy(hc.begin(), hc.end(), res.core);
+  }
+  if (res.factor) {
+    SPB_CUDA(cudaMemcpyAsync(res.factor, U.p, sizeof(double) * n * r, cudaMemcpyDeviceToHost, st));
+  }
+  SPB_CUDA(cudaStreamSynchronize(st));
+  res.time_ms = tall.stop_ms();
+  (void)wall0;
+  res.s3ttmc_ms = s3_ms;
+  res.dense_ms = dense_ms;
+  res.iterations = iters;
+  res.error = error;
+  res.core_norm = std::sqrt(cn2);
+  return status;
+}
+
+// hoevd: U = top-r eigenvectors of A = X_(1) X_(1)^T built on the device
+// from the leaf-grouped owners (src/sparse/spsymtensor.cpp:363-382).
+void hoevd_factor(TensorState &t, cudaStream_t st, int r, double *U, bool print_matrix) {
+  const int n = (int)t.dim;
+  if ((uint64_t)n * n > (1ull << 31))
+    fail(SYMPROP_ERR_SIZE, "hoevd: dense n x n matrix for n=%d is too large", n);
+  tree_build(t);
+  const TreeLevels &tr = *t.tree;
+  const uint32_t lv = tr.depth - 1;
+  DBuf<double> A((size_t)n * n);
+  SPB_CUDA(cudaMemsetAsync(A.p, 0, sizeof(double) * n * n, st));
+  uint64_t nleaf = tr.size[lv];
+  if (nleaf) {
+    hoevd_syrk_kernel<<<(unsigned)((nleaf + 127) / 128), 128, 0, st>>>(
+        tr.level_ptr[lv].p, tr.own_rem.p, tr.own_val.p, tr.leaf_mult.p, nleaf, n, A.p);
+    SPB_LAUNCH_CHECK();
+  }
+  if (print_matrix) {
+    std::vector<double> h((size_t)n * n);
+    SPB_CUDA(cudaMemcpyAsync(h.data(), A.p, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, st));
+    SPB_CUDA(cudaStreamSynchronize(st));
+    for (int i = 0; i < n; i++) {
+      for (int j = 0; j < n; j++) std::cout << h[(size_t)i * n + j] << ",";
+      std::cout << "\n";
+    }
+  }
+  std::vector<double> lam(r);
+  int e = dense::top_eigs(st, A.p, n, r, U, lam.data(), nullptr, 1e-12, 100);
+  if (e != SYMPROP_OK) std::printf("Eigendecomposition failed to converge.\n");
+}
+
+}  // namespace spb
+
+extern "C" int symprop_tucker(const symprop_tensor *t, const symprop_config *cfg, int alg,
+                              symprop_result *res) {
+  int st = SYMPROP_OK;
+  int g = spb::guard([&] {
+    if (!t || !cfg || !res) spb::fail(SYMPROP_ERR_INVALID, "null argument");
+    SPB_CUDA(cudaSetDevice(t->s.device));
+    st = spb::run_tucker(const_cast<spb::TensorState &>(t->s), *cfg, alg, *res);
+  });
+  if (g != SYMPROP_OK) return g;
+  if (st != SYMPROP_OK) {
+    spb::set_last_error("eigensolver did not reach its tolerance (results returned)");
+  }
+  return st;
 }

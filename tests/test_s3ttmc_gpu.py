@@ -37,11 +37,19 @@ def test_golden_outputs_fp64_and_fp32(gpu):
         assert rel(Y32.astype(np.float64), g[f"c{ci}_Yp"]) < FP32_TOL, (ci, rel(Y32, g[f"c{ci}_Yp"]))
 
 
+@pytest.fixture(params=[1, 2], ids=["rows", "tiled"])
+def schedule(request, gpu):
+    assert gpu.lib().symprop_s3ttmc_schedule(request.param) == 0
+    yield request.param
+    gpu.lib().symprop_s3ttmc_schedule(0)
+
+
 @pytest.mark.parametrize("order,n,nnz,R,s", [
     (3, 200, 3000, 8, 1.2), (4, 500, 20000, 16, 1.1), (5, 250, 10000, 8, 1.2),
     (6, 60, 4000, 4, 1.3), (7, 20, 500, 3, 1.2), (4, 50, 30000, 5, 1.5),
+    (5, 120, 6000, 16, 1.1), (6, 200, 3000, 10, 1.1), (4, 300, 8000, 13, 1.2),
 ])
-def test_against_oracle(gpu, order, n, nnz, R, s):
+def test_against_oracle(gpu, schedule, order, n, nnz, R, s):
     t = synth.zipf_tuples(order, n, nnz, s, 100 + order)
     v = synth.uniform_values(nnz, 5)
     U = np.random.default_rng(order).standard_normal((n, R))
@@ -54,7 +62,7 @@ def test_against_oracle(gpu, order, n, nnz, R, s):
     assert X.norm() == pytest.approx(orc.norm(order, t, v), rel=1e-13)
 
 
-def test_hub_row_split_is_deterministic(gpu):
+def test_hub_row_split_is_deterministic(gpu, schedule):
     # one id in every tuple: its row is cut into many slices whose partials
     # are combined in a fixed order
     rng = np.random.default_rng(7)
