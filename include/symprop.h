@@ -184,6 +184,39 @@ int symprop_write_decomp(const char *path, const double *core,
                          const double *factor, uint32_t dim, uint32_t rank,
                          uint32_t order, int append);
 
+/* --------------------------------------------------- learned warm start */
+/* No counterpart in the reference, which starts from random factors
+ * (src/tucker.cpp:25-36) or hoevd/hosvd (src/sparse/spsymtensor.cpp:339-383).
+ * A per-node MLP (F = R+2 inputs -> H hidden (ReLU) -> R outputs) maps node
+ * features to an initial factor; weights are one flat array
+ * [W1 (H x F), b1 (H), W2 (R x H), b2 (R)] of P = H*F + H + R*H + R values.
+ * All pointers below are device pointers except where marked host. */
+
+/* dX (dim x (R+2), FP32): standardised [log1p(degree), log1p(weighted
+ * degree), R-column sketch Y D^1/2 Omega of one S3TTMc pass with a Gaussian
+ * factor]; `seed` fixes the Gaussian draws. */
+int symprop_ws_features(const symprop_tensor *t, uint32_t R, uint64_t seed, float *dX, void *stream);
+/* forward: dZ1 (n x H) pre-activations, dOut (n x O); weights in BF16 */
+int symprop_mlp_forward(const float *dX, uint32_t n, uint32_t F, uint32_t H, uint32_t O,
+                        const void *dW_bf16, float *dZ1, float *dOut, void *stream);
+/* backward: dgrad (P, FP32) = dL/dW for dL/dOut = dgOut (n x O) */
+int symprop_mlp_backward(const float *dX, uint32_t n, uint32_t F, uint32_t H, uint32_t O,
+                         const void *dW_bf16, const float *dZ1, const float *dgOut, float *dgrad,
+                         void *stream);
+/* rotation-invariant projector loss L = r - tr(P_label P_out) with
+ * P_out = X (X^T X)^-1 X^T, X = dOut (n x r); dUlabel n x r orthonormal
+ * (FP64); writes dL/dX to dgOut and L to *loss (host). */
+int symprop_projector_loss(const float *dOut, const double *dUlabel, uint32_t n, uint32_t r,
+                           float *dgOut, double *loss, void *stream);
+/* Adam on the FP32 master weights; refreshes the BF16 shadow dw_bf16. */
+int symprop_adam_step(float *dw, float *dm, float *dv, const float *dg, uint32_t P, float lr,
+                      float beta1, float beta2, float eps, uint32_t step, void *dw_bf16,
+                      void *stream);
+/* Initial factor for a tensor: features -> MLP (host FP32 weights hW, H
+ * hidden) -> orthonormal basis; writes dim x R doubles to host hU. */
+int symprop_ws_predict(const symprop_tensor *t, uint32_t R, uint64_t seed, uint32_t H,
+                       const float *hW, double *hU);
+
 /* ------------------------------------------------------------- devices */
 int symprop_device_count(int *count);
 int symprop_set_device(int device);

@@ -221,15 +221,19 @@ __global__ void chol_inv_kernel(const double *G, int c, double *Rinv, int *statu
 
 // ---------------------------------------------------- Householder (1 CTA)
 
+// deterministic block reduction (warp shuffles, fixed tree); red >= 33 doubles
 __device__ double block_sum(double v, double *red) {
-  const int tid = threadIdx.x;
-  red[tid] = v;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  if (lane == 0) red[warp] = v;
   __syncthreads();
-  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
-    if (tid < s) red[tid] += red[tid + s];
-    __syncthreads();
+  if (warp == 0) {
+    double w = lane < nw ? red[lane] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) w += __shfl_down_sync(0xffffffffu, w, o);
+    if (lane == 0) red[32] = w;
   }
-  double r = red[0];
+  __syncthreads();
+  double r = red[32];
   __syncthreads();
   return r;
 }
@@ -542,7 +546,9 @@ bool orthonormalize(cudaStream_t st, double *A, int rows, int cols) {
     return true;
   }
   Scratch G(sizeof(double) * cols * cols, st), Ri(sizeof(double) * cols * cols, st),
-      tmp(sizeof(double) * (size_t)rows * cols, st), stat(sizeof(int) * 2, st);
+      tmp(sizeof(double) * (size_t)rows * cols, st), stat(sizeof(int) * 2, st),
+      orig(sizeof(double) * (size_t)rows * cols, st);
+  SPB_CUDA(cudaMemcpyAsync(orig.p, A, sizeof(double) * (size_t)rows * cols, cudaMemcpyDeviceToDevice, st));
   int hstat[2] = {0, 0};
   for (int pass = 0; pass < 2; ++pass) {
     gemm<double>(st, cols, cols, rows, 1.0, A, cols, true, A, cols, false, 0.0, G.as<double>(), cols,
@@ -559,15 +565,23 @@ bool orthonormalize(cudaStream_t st, double *A, int rows, int cols) {
   SPB_CUDA(cudaMemcpyAsync(hstat, stat.p, sizeof(int) * 2, cudaMemcpyDeviceToHost, st));
   SPB_CUDA(cudaStreamSynchronize(st));
   if (hstat[0] || hstat[1]) {
-    // numerically singular: the first pass already mixed in garbage, but
-    // Householder of the result still spans a valid orthonormal set; redo
-    // from the mixed columns is acceptable only if we keep the span, so the
-    // caller's original columns are not available here.  Householder on the
-    // current A gives an orthonormal basis of its (rank-completed) span.
+    // Gram matrix numerically singular: restart from the original columns
+    // with Householder QR, which is stable for any conditioning.
+    SPB_CUDA(cudaMemcpyAsync(A, orig.p, sizeof(double) * (size_t)rows * cols, cudaMemcpyDeviceToDevice, st));
     householder_q(st, A, rows, cols);
     return true;
   }
   return false;
+}
+
+// W -= Q (Q^T W) twice (classical Gram-Schmidt with re-orthogonalisation)
+static void project_out(cudaStream_t st, const double *Q, int ldq, int width, double *W, int s, int b,
+                        double *C) {
+  if (width <= 0) return;
+  for (int pass = 0; pass < 2; ++pass) {
+    gemm<double>(st, width, b, s, 1.0, Q, ldq, true, W, b, false, 0.0, C, b);
+    gemm<double>(st, s, b, width, -1.0, Q, ldq, false, C, b, false, 1.0, W, b);
+  }
 }
 
 void jacobi_eig(cudaStream_t st, const double *S, int n, double *w, double *V) {
@@ -631,39 +645,25 @@ int top_eigs(cudaStream_t st, const double *S, int s, int r, double *V, double *
     SPB_LAUNCH_CHECK();
   }
   std::vector<double> hw(nb), hres(b);
-  uint64_t reseed = 1;
   for (int it = 0; it <= max_restarts; ++it) {
     // Q[:, 0:b] = orth(X)
     copy_cols_kernel<<<cdiv((long long)s * b, 256), 256, 0, st>>>(X.as<double>(), b, s, b,
                                                                   blk.as<double>(), b);
     SPB_LAUNCH_CHECK();
-    orthonormalize(st, blk.as<double>(), s, b);
+    householder_q(st, blk.as<double>(), s, b);
     copy_cols_kernel<<<cdiv((long long)s * b, 256), 256, 0, st>>>(blk.as<double>(), b, s, b, q, nb);
     SPB_LAUNCH_CHECK();
     int width = b;
     for (int j = 1; j < nblk; ++j) {
-      // W = S * Q[:, (j-1)b : jb]
+      // W = S * Q[:, (j-1)b : jb], orthogonalised against the basis so far.
+      // Krylov blocks are badly scaled (columns follow the spectrum), so
+      // they are orthonormalised with Householder QR; a second projection
+      // removes any direction Householder invented for a rank-deficient W.
       gemm<double>(st, s, b, s, 1.0, S, s, false, q + (j - 1) * b, nb, false, 0.0, blk.as<double>(), b);
-      for (int pass = 0; pass < 2; ++pass) {  // W -= Q (Q^T W)
-        gemm<double>(st, width, b, s, 1.0, q, nb, true, blk.as<double>(), b, false, 0.0,
-                     C.as<double>(), b);
-        gemm<double>(st, s, b, width, -1.0, q, nb, false, C.as<double>(), b, false, 1.0,
-                     blk.as<double>(), b);
-      }
-      bool hh = orthonormalize(st, blk.as<double>(), s, b);
-      if (hh) {
-        // breakdown: continue the basis with fresh directions
-        random_fill_kernel<<<cdiv((long long)s * b, 256), 256, 0, st>>>(blk.as<double>(),
-                                                                         (size_t)s * b, ++reseed);
-        SPB_LAUNCH_CHECK();
-        for (int pass = 0; pass < 2; ++pass) {
-          gemm<double>(st, width, b, s, 1.0, q, nb, true, blk.as<double>(), b, false, 0.0,
-                       C.as<double>(), b);
-          gemm<double>(st, s, b, width, -1.0, q, nb, false, C.as<double>(), b, false, 1.0,
-                       blk.as<double>(), b);
-        }
-        orthonormalize(st, blk.as<double>(), s, b);
-      }
+      project_out(st, q, nb, width, blk.as<double>(), s, b, C.as<double>());
+      householder_q(st, blk.as<double>(), s, b);
+      project_out(st, q, nb, width, blk.as<double>(), s, b, C.as<double>());
+      householder_q(st, blk.as<double>(), s, b);
       copy_cols_kernel<<<cdiv((long long)s * b, 256), 256, 0, st>>>(blk.as<double>(), b, s, b,
                                                                     q + j * b, nb);
       SPB_LAUNCH_CHECK();

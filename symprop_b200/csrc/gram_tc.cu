@@ -288,7 +288,7 @@ __global__ void symmetrize_kernel(const float *G, int m, double *S) {
   size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= (size_t)m * m) return;
   int i = (int)(idx / m), j = (int)(idx % m);
-  bool upper = (i / TM) <= (j / TN);
+  bool upper = i <= j;  // upper tiles are complete; i <= j also fixes the diagonal tiles
   S[idx] = (double)(upper ? G[idx] : G[(size_t)j * m + i]);
 }
 

@@ -87,6 +87,9 @@ template <> struct Vec4<double> {
   }
 };
 
+// number of terms of the deepest DP level (levels 2..L-1 have d terms)
+__host__ __device__ constexpr int d_max(int L) { return L > 2 ? L - 1 : 1; }
+
 template <int L, int NT, typename T>
 __global__ void __launch_bounds__(kThreads, 2) s3ttmc_tiled_kernel(const TiledParams p) {
   constexpr bool kExact = sizeof(T) == 8;
@@ -148,39 +151,60 @@ __global__ void __launch_bounds__(kThreads, 2) s3ttmc_tiled_kernel(const TiledPa
 
   for (uint64_t ob = ch.ob; ob < ch.oe; ob += BO) {
     const uint32_t nb = (uint32_t)min((uint64_t)BO, ch.oe - ob);
-    // stage U rows and coefficient-scaled rows of the batch
+    // stage U rows and coefficient-scaled rows of the batch; the flat index
+    // i = (o*L + k)*R4 + x advances by kThreads with carries (no division
+    // inside the loop)
     const uint32_t per = L * R4;
-    for (uint32_t i = tid; i < nb * per; i += kThreads) {
-      uint32_t o = i / per, rem = i - o * per, k = rem / R4, x = rem - k * R4;
-      T u = T(0);
-      if (x < R) u = U[(uint64_t)p.own_S[(ob + o) * p.sstride + k] * R + x];
-      sU[i] = u;
-      sW[i] = own_c[ob + o] * u;
+    {
+      uint32_t o = (uint32_t)tid / per, rem = (uint32_t)tid - o * per, k = rem / R4, x = rem - k * R4;
+      const uint32_t dO = kThreads / per, dr = kThreads - dO * per, dK = dr / R4, dX = dr - dK * R4;
+      while (o < nb) {
+        const uint32_t i = o * per + k * R4 + x;
+        T u = T(0);
+        if (x < R) u = U[(uint64_t)p.own_S[(ob + o) * p.sstride + k] * R + x];
+        sU[i] = u;
+        sW[i] = own_c[ob + o] * u;
+        x += dX;
+        if (x >= R4) { x -= R4; ++k; }
+        k += dK;
+        if (k >= (uint32_t)L) { k -= L; ++o; }
+        o += dO;
+      }
     }
     __syncthreads();
-    // intermediate sub-multiset tensors (colex), levels 2 .. L-1
+    // intermediate sub-multiset tensors (colex), levels 2 .. L-1; item
+    // (o, mask, e) advances by kThreads with carries
 #pragma unroll 1
     for (int d = 2; d < L; ++d) {
       const uint32_t md = p.m[d], md4 = p.m4[d], nd = p.desc_count[d];
-      const uint32_t items = nb * nd * md4;
       const uint8_t *jt = sJ + p.jtab_off[d];
-      const uint32_t *st = sStart + d * (R + 1);
-      for (uint32_t it = tid; it < items; it += kThreads) {
-        uint32_t o = it / (nd * md4), rem = it - o * nd * md4, mi = rem / md4, e = rem - mi * md4;
-        const DpDesc &ds = sDesc[p.desc_begin[d] + mi];
+      const uint32_t *stt = sStart + d * (R + 1);
+      const DpDesc *dd = sDesc + p.desc_begin[d];
+      const uint32_t perd = nd * md4;
+      uint32_t o = (uint32_t)tid / perd, rem = (uint32_t)tid - o * perd, mi = rem / md4, e = rem - mi * md4;
+      const uint32_t dO = kThreads / perd, dr = kThreads - dO * perd, dM = dr / md4, dE = dr - dM * md4;
+      while (o < nb) {
+        const DpDesc &ds = dd[mi];
         T v = T(0);
         if (e < md) {
-          uint32_t j = jt[e];
-          uint32_t r = e - st[j];
+          const uint32_t j = jt[e];
+          const uint32_t r = e - stt[j];
           const T *uo = sU + (size_t)o * per;
           const T *ko = sK + (size_t)o * p.ksz4;
-          for (uint32_t t = 0; t < ds.nterm; ++t) {
-            uint32_t s = ds.src[t];
-            T a = (s & kURow) ? uo[(s & 0xffu) * R4 + r] : ko[s + r];
+#pragma unroll
+          for (int t = 0; t < d_max(L); ++t) {
+            if (t >= d) break;
+            const uint32_t s = ds.src[t];
+            const T a = (s & kURow) ? uo[(s & 0xffu) * R4 + r] : ko[s + r];
             v += a * uo[ds.k[t] * R4 + j];
           }
         }
         sK[(size_t)o * p.ksz4 + ds.dst + e] = v;
+        e += dE;
+        if (e >= md4) { e -= md4; ++mi; }
+        mi += dM;
+        if (mi >= nd) { mi -= nd; ++o; }
+        o += dO;
       }
       __syncthreads();
     }

@@ -87,6 +87,14 @@ void regularize(cudaStream_t st, double *U, int n, int r, double delta) {
   dense::orthonormalize(st, U, n, r);  // leftsvd(U) -> any orthonormal basis of its span
 }
 
+// The reference prints LAPACK's failure and carries on with the result
+// (src/dense/matrixops.cpp:31-33, 86-89); the eigensolver here does the same.
+void warn_noconv(int alg) {
+  std::printf(alg == SYMPROP_ALTHOOI ? "Eigendecomposition failed to converge.\n"
+                                     : "SVD failed to converge.\n");
+  std::fflush(stdout);
+}
+
 }  // namespace
 
 void hoevd_factor(TensorState &t, cudaStream_t st, int r, double *U, bool print_matrix);
@@ -209,7 +217,7 @@ int run_tucker(TensorState &t, const symprop_config &c, int alg, symprop_result 
         }
         int e = dense::top_eigs(st, S.p, n, r, V.p, lam.data(), have_warm ? Vwarm.p : nullptr,
                                 eig_tol, 60);
-        if (e != SYMPROP_OK) status = e;
+        if (e != SYMPROP_OK) warn_noconv(alg);
         SPB_CUDA(cudaMemcpyAsync(U.p, V.p, sizeof(double) * n * r, cudaMemcpyDeviceToDevice, st));
       } else {
         if (mixed) {
@@ -222,7 +230,7 @@ int run_tucker(TensorState &t, const symprop_config &c, int alg, symprop_result 
         }
         int e = dense::top_eigs(st, S.p, m, r, V.p, lam.data(), have_warm ? Vwarm.p : nullptr,
                                 eig_tol, 60);
-        if (e != SYMPROP_OK) status = e;
+        if (e != SYMPROP_OK) warn_noconv(alg);
         if (mixed) {
           dense::convert<double, float>(st, V.p, V32.p, (size_t)m * r);
           dense::gemm<float>(st, n, r, m, 1.f, Y32.p, m, false, V32.p, r, false, 0.f, W32.p, r, sD32.p);

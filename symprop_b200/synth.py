@@ -123,6 +123,43 @@ def powerlaw_communities(order: int, n: int, nnz: int, gamma: float,
     return _draw_unique(draw, nnz, order, rng)
 
 
+def community_zipf(order: int, n: int, nnz: int, communities: int, s: float, seed: int,
+                   frac_in: float = 0.9) -> np.ndarray:
+    """Planted communities with Zipf(s) degrees inside each community: a
+    fraction frac_in of the tuples draw all ids from one community (ranked by
+    a seeded permutation), the rest draw ids Zipf(s) over all nodes."""
+    rng = np.random.default_rng(seed)
+    comm = rng.integers(0, communities, size=n)
+    members = [np.nonzero(comm == c)[0] for c in range(communities)]
+    members = [m if len(m) else np.array([c % n]) for c, m in enumerate(members)]
+    cdfs = []
+    for mem in members:
+        w = np.arange(1, len(mem) + 1, dtype=np.float64) ** (-s)
+        c = np.cumsum(w)
+        cdfs.append(c / c[-1])
+        rng.shuffle(mem)
+    wall = np.arange(1, n + 1, dtype=np.float64) ** (-s)
+    call = np.cumsum(wall)
+    call /= call[-1]
+    perm = rng.permutation(n)
+
+    def draw(k):
+        t = perm[np.minimum(np.searchsorted(call, rng.random((k, order)), side="right"), n - 1)].astype(np.int64)
+        inside = rng.random(k) < frac_in
+        cs = rng.integers(0, communities, size=k)
+        for c in range(communities):
+            sel = inside & (cs == c)
+            cnt = int(sel.sum())
+            if not cnt:
+                continue
+            idx = np.minimum(np.searchsorted(cdfs[c], rng.random((cnt, order)), side="right"),
+                             len(members[c]) - 1)
+            t[sel] = members[c][idx]
+        return t.astype(np.uint32)
+
+    return _draw_unique(draw, nnz, order, rng)
+
+
 def uniform_values(nnz: int, seed: int) -> np.ndarray:
     """values uniform in (0, 1], rounded to float32 and widened (exact in FP64)."""
     rng = np.random.default_rng(seed + 7919)
