@@ -110,9 +110,11 @@ int symprop_s3ttmc(const symprop_tensor *t, const void *U, uint32_t R,
 int symprop_s3ttmc_device(const symprop_tensor *t, const void *dU, uint32_t R,
                           int packed, void *dY, int precision, void *stream);
 /* Selects the S3TTMc schedule for the whole process: 0 automatic (default:
- * register-tiled where the shape is supported), 1 per-owner rows kernel,
- * 2 register-tiled only.  Both compute the same Y; tests use this to check
- * each schedule against the oracle. */
+ * warp-per-owner where the packed output fits one warp's registers, else
+ * CTA register-tiled, else the per-owner rows kernel), 1 rows kernel,
+ * 2 CTA register-tiled only, 3 warp-per-owner only (2 and 3 return
+ * SYMPROP_ERR_SIZE on shapes they do not cover).  All compute the same Y;
+ * tests use this to check each schedule against the oracle. */
 int symprop_s3ttmc_schedule(int schedule);
 /* Number of kernel launches one symprop_s3ttmc_device call issues for
  * (R, packed); lets callers count their launches. */

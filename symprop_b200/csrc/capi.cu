@@ -201,7 +201,7 @@ int symprop_s3ttmc(const symprop_tensor *t, const void *U, uint32_t R, int packe
 
 int symprop_s3ttmc_schedule(int schedule) {
   return guard([&] {
-    require(schedule >= 0 && schedule <= 2, "schedule must be 0, 1 or 2");
+    require(schedule >= 0 && schedule <= 3, "schedule must be 0, 1, 2 or 3");
     set_s3ttmc_schedule(schedule);
   });
 }

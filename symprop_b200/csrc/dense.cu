@@ -166,15 +166,23 @@ __global__ void sum_pairs_kernel(const double *part, int n, double *out) {
 
 // ------------------------------------------------------------ Cholesky
 
-// G (c x c) -> Rinv (upper-triangular inverse of the Cholesky factor R,
-// G = R^T R).  status[0] = 1 when a pivot is not safely positive.
+// G (c x c) -> Rinv with A Rinv orthonormal for G = A^T A.  The columns are
+// first scaled to unit norm (G' = D G D, D = diag(G)^-1/2), so the pivot test
+// measures linear dependence, not column scaling; Rinv = D R'^-1 with
+// G' = R'^T R'.  status[0] = 1 when a pivot is not safely positive.
 __global__ void chol_inv_kernel(const double *G, int c, double *Rinv, int *status) {
   extern __shared__ double sm[];
   double *R = sm;          // c x c
   double *Ri = sm + c * c; // c x c
+  __shared__ double dsc[64];
   const int tid = threadIdx.x, nt = blockDim.x;
+  for (int i = tid; i < c; i += nt) {
+    double g = G[i * c + i];
+    dsc[i] = g > 0 ? 1.0 / sqrt(g) : 1.0;
+  }
+  __syncthreads();
   for (int i = tid; i < c * c; i += nt) {
-    R[i] = G[i];
+    R[i] = G[i] * dsc[i / c] * dsc[i % c];
     Ri[i] = 0.0;
   }
   __syncthreads();
@@ -215,7 +223,7 @@ __global__ void chol_inv_kernel(const double *G, int c, double *Rinv, int *statu
     }
   }
   __syncthreads();
-  for (int i = tid; i < c * c; i += nt) Rinv[i] = Ri[i];
+  for (int i = tid; i < c * c; i += nt) Rinv[i] = Ri[i] * dsc[i / c];
   if (tid == 0) status[0] = bad;
 }
 
@@ -650,20 +658,21 @@ int top_eigs(cudaStream_t st, const double *S, int s, int r, double *V, double *
     copy_cols_kernel<<<cdiv((long long)s * b, 256), 256, 0, st>>>(X.as<double>(), b, s, b,
                                                                   blk.as<double>(), b);
     SPB_LAUNCH_CHECK();
-    householder_q(st, blk.as<double>(), s, b);
+    orthonormalize(st, blk.as<double>(), s, b);
     copy_cols_kernel<<<cdiv((long long)s * b, 256), 256, 0, st>>>(blk.as<double>(), b, s, b, q, nb);
     SPB_LAUNCH_CHECK();
     int width = b;
     for (int j = 1; j < nblk; ++j) {
-      // W = S * Q[:, (j-1)b : jb], orthogonalised against the basis so far.
-      // Krylov blocks are badly scaled (columns follow the spectrum), so
-      // they are orthonormalised with Householder QR; a second projection
-      // removes any direction Householder invented for a rank-deficient W.
+      // W = S * Q[:, (j-1)b : jb], orthogonalised against the basis so far
+      // (column-scaled CholQR2; Householder when W is numerically rank
+      // deficient, then a second projection removes any direction it
+      // invented inside the existing basis).
       gemm<double>(st, s, b, s, 1.0, S, s, false, q + (j - 1) * b, nb, false, 0.0, blk.as<double>(), b);
       project_out(st, q, nb, width, blk.as<double>(), s, b, C.as<double>());
-      householder_q(st, blk.as<double>(), s, b);
-      project_out(st, q, nb, width, blk.as<double>(), s, b, C.as<double>());
-      householder_q(st, blk.as<double>(), s, b);
+      if (orthonormalize(st, blk.as<double>(), s, b)) {
+        project_out(st, q, nb, width, blk.as<double>(), s, b, C.as<double>());
+        householder_q(st, blk.as<double>(), s, b);
+      }
       copy_cols_kernel<<<cdiv((long long)s * b, 256), 256, 0, st>>>(blk.as<double>(), b, s, b,
                                                                     q + j * b, nb);
       SPB_LAUNCH_CHECK();

@@ -22,6 +22,7 @@
 #include <cstdlib>
 
 #include "s3ttmc_tiled.cuh"
+#include "s3ttmc_warp.cuh"
 #include "tensor.cuh"
 
 namespace spb {
@@ -310,15 +311,26 @@ __global__ void __launch_bounds__(256, 1) s3ttmc_rows_kernel(const RowParams p) 
 }
 
 // rows cut into slices: add the FP64 partials in slot order
+// grid (split rows, column blocks of 32): warp w adds slots w, w+8, ... for
+// 32 consecutive columns (coalesced), then the 8 warp sums are added in
+// warp order (deterministic)
 template <typename T>
-__global__ void combine_kernel(const SplitRow *split, const double *partials, uint32_t mL,
-                               void *Yv, uint64_t ldy) {
+__global__ void __launch_bounds__(256) combine_kernel(const SplitRow *split, const double *partials,
+                                                      uint32_t mL, void *Yv, uint64_t ldy) {
+  __shared__ double red[8][32];
   const SplitRow s = split[blockIdx.x];
-  T *Y = reinterpret_cast<T *>(Yv) + (uint64_t)s.row * ldy;
-  for (uint32_t q = threadIdx.x; q < mL; q += blockDim.x) {
-    double a = 0.0;
-    for (uint32_t k = s.slot_begin; k < s.slot_end; ++k) a += partials[(uint64_t)k * mL + q];
-    Y[q] = (T)a;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t q = blockIdx.y * 32 + lane;
+  double a = 0.0;
+  if (q < mL)
+    for (uint32_t k = s.slot_begin + warp; k < s.slot_end; k += 8) a += partials[(uint64_t)k * mL + q];
+  red[warp][lane] = a;
+  __syncthreads();
+  if (warp == 0 && q < mL) {
+    double t = 0.0;
+#pragma unroll
+    for (int w = 0; w < 8; ++w) t += red[w][lane];
+    reinterpret_cast<T *>(Yv)[(uint64_t)s.row * ldy + q] = (T)t;
   }
 }
 
@@ -457,7 +469,18 @@ void s3ttmc_run(TensorState &t, const void *dU, uint32_t R, bool packed, void *d
   }
   if (t.nslots) t.partials.ensure((size_t)t.nslots * m);
   const int sched = s3ttmc_schedule();
-  if (sched != kScheduleRows) {
+  if (sched == kScheduleAuto || sched == kScheduleWarp) {
+    auto it = t.warp.find(R);
+    if (it == t.warp.end()) it = t.warp.emplace(R, warp_plan(t.order, R)).first;
+    if (warp_supported(*it->second)) {
+      warp_launch(*it->second, t, dU, Ypk, precision, st);
+      finish_rows(t, m, Ypk, packed, dY, R, L, precision, st);
+      return;
+    }
+    if (sched == kScheduleWarp)
+      fail(SYMPROP_ERR_SIZE, "warp S3TTMc does not support order %u rank %u", t.order, R);
+  }
+  if (sched == kScheduleAuto || sched == kScheduleTiled) {
     auto it = t.tiled.find(R);
     if (it == t.tiled.end()) it = t.tiled.emplace(R, tiled_plan(t.order, R)).first;
     if (tiled_supported(*it->second)) {
@@ -509,10 +532,11 @@ void s3ttmc_run(TensorState &t, const void *dU, uint32_t R, bool packed, void *d
 static void finish_rows(TensorState &t, uint64_t m, void *Ypk, bool packed, void *dY, uint32_t R,
                         uint32_t L, int precision, cudaStream_t st) {
   if (t.nsplit) {
+    dim3 grid(t.nsplit, (unsigned)((m + 31) / 32));
     if (precision == SYMPROP_FP64)
-      combine_kernel<double><<<t.nsplit, 256, 0, st>>>(t.split.p, t.partials.p, (uint32_t)m, Ypk, m);
+      combine_kernel<double><<<grid, 256, 0, st>>>(t.split.p, t.partials.p, (uint32_t)m, Ypk, m);
     else
-      combine_kernel<float><<<t.nsplit, 256, 0, st>>>(t.split.p, t.partials.p, (uint32_t)m, Ypk, m);
+      combine_kernel<float><<<grid, 256, 0, st>>>(t.split.p, t.partials.p, (uint32_t)m, Ypk, m);
     SPB_LAUNCH_CHECK();
   }
   if (!packed) unpack_rows(Ypk, t.dim, R, L, dY, precision, st);

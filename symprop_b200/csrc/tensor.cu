@@ -252,6 +252,8 @@ void tensor_build(TensorState &t, const uint32_t *h_inds, const double *h_vals) 
     return (a.oe - a.ob) > (b.oe - b.ob);
   });
   t.nchunks = (uint32_t)ch.size();
+  t.nheavy = 0;
+  while (t.nheavy < t.nchunks && ch[t.nheavy].oe - ch[t.nheavy].ob > kLightOwners) ++t.nheavy;
   t.nsplit = (uint32_t)sp.size();
   t.nslots = slot;
   t.chunks.alloc(ch.size());

@@ -36,6 +36,9 @@ struct Chunk {
   uint64_t ob, oe;
 };
 static constexpr uint32_t kDirect = 0xffffffffu;
+// work items with at most this many owners take one warp each in the
+// warp-per-owner S3TTMc schedule (larger ones take a whole CTA)
+static constexpr uint32_t kLightOwners = 48;
 
 struct SplitRow {
   uint32_t row;
@@ -60,10 +63,12 @@ struct TreeLevels {
 // register-tiled schedule (s3ttmc_tiled.cu).
 struct PackedTables;
 struct TiledPlan;
+struct WarpPlan;
 
-// S3TTMc schedule: 0 = automatic (tiled where supported), 1 = per-owner
-// rows kernel, 2 = tiled (error if unsupported).
-enum { kScheduleAuto = 0, kScheduleRows = 1, kScheduleTiled = 2 };
+// S3TTMc schedule: 0 = automatic (warp, else tiled, else rows), 1 = per-owner
+// rows kernel, 2 = CTA register-tiled, 3 = warp per owner (2 and 3 fail on
+// shapes they do not support).
+enum { kScheduleAuto = 0, kScheduleRows = 1, kScheduleTiled = 2, kScheduleWarp = 3 };
 int s3ttmc_schedule();
 void set_s3ttmc_schedule(int s);
 
@@ -86,6 +91,7 @@ struct TensorState {
 
   uint32_t chunk_owners = 0;  // max owners per chunk
   uint32_t nchunks = 0;
+  uint32_t nheavy = 0;        // leading chunks with more than kLightOwners owners
   DBuf<Chunk> chunks;
   uint32_t nsplit = 0, nslots = 0;
   DBuf<SplitRow> split;
@@ -96,6 +102,7 @@ struct TensorState {
 
   std::map<uint32_t, std::shared_ptr<PackedTables>> tables;  // by R
   std::map<uint32_t, std::shared_ptr<TiledPlan>> tiled;      // by R
+  std::map<uint32_t, std::shared_ptr<WarpPlan>> warp;        // by R
   std::unique_ptr<TreeLevels> tree;
 };
 

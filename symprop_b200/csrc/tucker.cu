@@ -182,7 +182,11 @@ int run_tucker(TensorState &t, const symprop_config &c, int alg, symprop_result 
   SPB_CUDA(cudaMemsetAsync(core_prev.p, 0, sizeof(double) * r * m, st));
   bool have_warm = false;
   std::vector<double> lam(r);
-  const double eig_tol = mixed ? 1e-7 : 1e-12;
+  // Mixed precision runs until |delta error| < max(tol, kMixedFloor), the
+  // resolution of its FP32/BF16 arithmetic, then finishes with FP64
+  // iterations so the final objective is the FP64 fixed point's.
+  constexpr double kMixedFloor = 1e-5;
+  bool mx = mixed;
 
   double prev_error = 0.0, error = 0.0, cn2 = 0.0;
   double s3_ms = 0, dense_ms = 0;
@@ -191,12 +195,13 @@ int run_tucker(TensorState &t, const symprop_config &c, int alg, symprop_result 
   const int prec_digits = alg == SYMPROP_ALTHOOI ? 10 : 12;
 
   for (uint64_t iter = 0; iter < c.max_iter; ++iter) {
+    const double eig_tol = mx ? 1e-7 : 1e-12;
     tphase.start();
     regularize(st, U.p, n, r, c.delta);
     dense_ms += tphase.stop_ms();
 
     tphase.start();
-    if (mixed) {
+    if (mx) {
       dense::convert<double, float>(st, U.p, U32.p, (size_t)n * r);
       s3ttmc_run(t, U32.p, (uint32_t)r, true, Y32.p, SYMPROP_FP32, st);
     } else {
@@ -209,7 +214,7 @@ int run_tucker(TensorState &t, const symprop_config &c, int alg, symprop_result 
     if (alg == SYMPROP_HOOI || alg == SYMPROP_ALTHOOI) {
       // leading r-dimensional left singular subspace of Y D^1/2
       if (gram_nn) {
-        if (mixed) {
+        if (mx) {
           dense::gemm<float>(st, n, n, m, 1.f, Y32.p, m, false, Y32.p, m, true, 0.f, S32.p, n, D32.p, true);
           dense::convert<float, double>(st, S32.p, S.p, (size_t)n * n);
         } else {
@@ -220,7 +225,7 @@ int run_tucker(TensorState &t, const symprop_config &c, int alg, symprop_result 
         if (e != SYMPROP_OK) warn_noconv(alg);
         SPB_CUDA(cudaMemcpyAsync(U.p, V.p, sizeof(double) * n * r, cudaMemcpyDeviceToDevice, st));
       } else {
-        if (mixed) {
+        if (mx) {
           // tcgen05 split-BF16 Gram of Y D^1/2 (FP32 accumulation)
           gram::gram_split_bf16(st, Y32.p, n, m, sD32.p, S.p, gram_ws.p, gram_err.p);
         } else {
@@ -231,7 +236,7 @@ int run_tucker(TensorState &t, const symprop_config &c, int alg, symprop_result 
         int e = dense::top_eigs(st, S.p, m, r, V.p, lam.data(), have_warm ? Vwarm.p : nullptr,
                                 eig_tol, 60);
         if (e != SYMPROP_OK) warn_noconv(alg);
-        if (mixed) {
+        if (mx) {
           dense::convert<double, float>(st, V.p, V32.p, (size_t)m * r);
           dense::gemm<float>(st, n, r, m, 1.f, Y32.p, m, false, V32.p, r, false, 0.f, W32.p, r, sD32.p);
           dense::convert<float, double>(st, W32.p, U.p, (size_t)n * r);
@@ -243,7 +248,7 @@ int run_tucker(TensorState &t, const symprop_config &c, int alg, symprop_result 
       SPB_CUDA(cudaMemcpyAsync(Vwarm.p, V.p, sizeof(double) * (size_t)s * r, cudaMemcpyDeviceToDevice, st));
       have_warm = true;
       // core = U^T Y (r x m packed)
-      if (mixed) {
+      if (mx) {
         dense::convert<double, float>(st, U.p, U32.p, (size_t)n * r);
         dense::gemm<float>(st, r, m, n, 1.f, U32.p, r, true, Y32.p, m, false, 0.f, core32.p, m);
         dense::convert<float, double>(st, core32.p, core.p, (size_t)r * m);
@@ -269,7 +274,7 @@ int run_tucker(TensorState &t, const symprop_config &c, int alg, symprop_result 
       SPB_CUDA(cudaStreamSynchronize(st));
       cn2 = h[1];
     } else {  // HOQRI
-      if (mixed) {
+      if (mx) {
         dense::convert<double, float>(st, U.p, U32.p, (size_t)n * r);
         dense::gemm<float>(st, r, m, n, 1.f, U32.p, r, true, Y32.p, m, false, 0.f, core32.p, m);
         dense::convert<float, double>(st, core32.p, core.p, (size_t)r * m);
@@ -289,7 +294,7 @@ int run_tucker(TensorState &t, const symprop_config &c, int alg, symprop_result 
       cn2 = h[1];
     }
     dense_ms += tphase.stop_ms();
-    if (mixed && !gram_nn) {
+    if (mx && !gram_nn) {
       int herr = 0;
       SPB_CUDA(cudaMemcpy(&herr, gram_err.p, sizeof(int), cudaMemcpyDeviceToHost));
       if (herr) fail(SYMPROP_ERR_TIMEOUT, "tensor-core Gram: a bounded wait expired");
@@ -309,7 +314,11 @@ int run_tucker(TensorState &t, const symprop_config &c, int alg, symprop_result 
       SPB_CUDA(cudaMemcpyAsync(core_prev.p, core.p, sizeof(double) * r * m, cudaMemcpyDeviceToDevice, st));
     }
     double error_diff = std::abs(prev_error - error);
-    if (error_diff < c.rel_tol) break;
+    if (mx && error_diff < std::max(c.rel_tol, kMixedFloor)) {
+      mx = false;  // continue in FP64 from the mixed-precision iterate
+    } else if (error_diff < c.rel_tol) {
+      break;
+    }
     prev_error = error;
     if (alg == SYMPROP_HOOI) {
       SPB_CUDA(cudaMemcpyAsync(core_prev.p, core.p, sizeof(double) * r * m, cudaMemcpyDeviceToDevice, st));

@@ -37,11 +37,21 @@ def test_golden_outputs_fp64_and_fp32(gpu):
         assert rel(Y32.astype(np.float64), g[f"c{ci}_Yp"]) < FP32_TOL, (ci, rel(Y32, g[f"c{ci}_Yp"]))
 
 
-@pytest.fixture(params=[1, 2], ids=["rows", "tiled"])
+@pytest.fixture(params=[1, 2, 3], ids=["rows", "tiled", "warp"])
 def schedule(request, gpu):
     assert gpu.lib().symprop_s3ttmc_schedule(request.param) == 0
     yield request.param
     gpu.lib().symprop_s3ttmc_schedule(0)
+
+
+def run_or_skip(gpu, schedule, fn):
+    """Schedules 2 and 3 reject shapes they do not cover with ERR_SIZE."""
+    try:
+        return fn()
+    except gpu.SympropError as e:
+        if schedule in (2, 3) and e.status == gpu.ERR_SIZE:
+            pytest.skip("shape not covered by this schedule")
+        raise
 
 
 @pytest.mark.parametrize("order,n,nnz,R,s", [
@@ -55,7 +65,7 @@ def test_against_oracle(gpu, schedule, order, n, nnz, R, s):
     U = np.random.default_rng(order).standard_normal((n, R))
     X = gpu.SpSymtensor(n, order, t, v)
     Yo = orc.s3ttmc(order, n, t, v, U, R, True)
-    Y = X.S3TTMc(U, R, True)
+    Y = run_or_skip(gpu, schedule, lambda: X.S3TTMc(U, R, True))
     assert rel(Y, Yo) < FP64_TOL
     Y32 = X.S3TTMc(U.astype(np.float32), R, True, precision=gpu.FP32)
     assert rel(Y32.astype(np.float64), Yo) < FP32_TOL
