@@ -143,6 +143,22 @@ int symprop_unpack_rows_device(const double *dpacked, uint64_t rows,
 int symprop_gram_device(const void *dY, uint64_t n, uint32_t m, const void *dscale,
                         double *dG, int precision, void *stream);
 
+/* The tensor-core (FP32-input) form of symprop_gram_device for callers that
+ * cannot allocate device memory at call time: services that reserve all
+ * device memory for their own pool allocator at start-up (a later cudaMalloc
+ * fails or fragments the pool), and code that must not take the implicit
+ * device synchronisation of cudaMalloc/cudaFree.  It allocates nothing: its
+ * workspace is one fixed 32 MiB device array inside this library, held by
+ * every GPU that loads the library until the process exits.  Inputs whose
+ * workspace (about 4*m*n + 4*m*m bytes) exceeds it are rejected with
+ * SYMPROP_ERR_SIZE.  The first call on each device looks the array up with
+ * that device current; make that first call before any stream capture.
+ * Every call reuses the same array, so calls that overlap on the GPU (other
+ * streams, other host threads) race and must be serialised by the caller.
+ * This entry point has no counterpart in the reference. */
+int symprop_gram_device_noalloc(const float *dY, uint64_t n, uint32_t m, const float *dscale,
+                                double *dG, void *stream);
+
 /* ------------------------------------------------------------- Tucker */
 typedef struct {
   uint32_t rank;      /* Config::rank     (include/detail/tucker.hpp:15) */

@@ -94,6 +94,7 @@ def lib():
         "symprop_write_decomp": (_I, [ctypes.c_char_p, _P, _P, _U32, _U32, _U32, _I]),
         "symprop_gram_device": (_I, [_P, _U64, _U32, _P, _P, _I, _P]),
         "symprop_s3ttmc_schedule": (_I, [_I]),
+        "symprop_gram_device_noalloc": (_I, [_P, _U64, _U32, _P, _P, _P]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

@@ -355,5 +355,98 @@ void gram_split_bf16(cudaStream_t st, const float *Y, int n, int m, const float 
   SPB_LAUNCH_CHECK();
 }
 
+// ---------------------------------------------------------------------------
+// Allocation-free variant.  Some callers cannot allocate device memory when
+// they call this library: services that reserve all device memory for their
+// own pool allocator at start-up (a later cudaMalloc fails or fragments the
+// pool), and code that must not pay cudaMalloc/cudaFree's implicit device
+// synchronisation.  For them the workspace of the tensor-core Gram lives in
+// one file-scope device array of kNoAllocBytes (32 MiB), which every GPU
+// that loads this library holds until the process exits.
+namespace {
+
+constexpr size_t kNoAllocBytes = 32ull << 20;
+__device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+// upper-triangular tile list written on the device (no host buffer)
+__global__ void fill_tiles_kernel(int2 *tiles, int nt) {
+  int id = blockIdx.x * blockDim.x + threadIdx.x;
+  int k = 0;
+  for (int i = 0; i < nt; ++i)
+    for (int j = i; j < nt; ++j, ++k)
+      if (k == id) tiles[id] = make_int2(i, j);
+}
+
+std::mutex g_noalloc_mu;
+void *g_noalloc_ptr[64] = {};
+
+// device address of the scratch array on the current device (looked up once
+// per device, with that device current)
+void *noalloc_scratch(int device) {
+  if (device < 0 || device >= 64) fail(SYMPROP_ERR_INVALID, "device id %d out of range", device);
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_ptr[device]) {
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p)
+      fail(SYMPROP_ERR_CUDA, "cudaGetSymbolAddress(g_noalloc_scratch) failed: %s", cudaGetErrorString(e));
+    g_noalloc_ptr[device] = p;
+  }
+  return g_noalloc_ptr[device];
+}
+
+}  // namespace
+
+size_t noalloc_capacity() { return kNoAllocBytes; }
+
+void gram_split_bf16_noalloc(cudaStream_t st, const float *Y, int n, int m, const float *sd, double *S) {
+  if (n <= 0 || m <= 0) fail(SYMPROP_ERR_INVALID, "n and m must be positive");
+  const size_t ldk = ((size_t)n + 63) / 64 * 64;
+  const int nt = (m + TM - 1) / TM;
+  const size_t ntiles = (size_t)nt * (nt + 1) / 2;
+  // layout: H | L | G (FP32) | tiles | error flag, each 256-byte aligned
+  auto up = [](size_t x) { return (x + 255) / 256 * 256; };
+  const size_t oH = 0, oL = up(oH + (size_t)m * ldk * 2), oG = up(oL + (size_t)m * ldk * 2),
+               oT = up(oG + (size_t)m * m * 4), oE = up(oT + ntiles * sizeof(int2)), need = oE + 256;
+  if (need > kNoAllocBytes)
+    fail(SYMPROP_ERR_SIZE,
+         "allocation-free Gram: n=%d, m=%d needs %zu bytes of scratch, the fixed array holds %zu", n, m,
+         need, kNoAllocBytes);
+  int dev = 0;
+  SPB_CUDA(cudaGetDevice(&dev));
+  unsigned char *w = (unsigned char *)noalloc_scratch(dev);
+  __nv_bfloat16 *H = (__nv_bfloat16 *)(w + oH), *L = (__nv_bfloat16 *)(w + oL);
+  float *G = (float *)(w + oG);
+  int2 *tiles = (int2 *)(w + oT);
+  int *err = (int *)(w + oE);
+  SPB_CUDA(cudaMemsetAsync(err, 0, sizeof(int), st));  // the array keeps the previous call's contents
+  fill_tiles_kernel<<<(unsigned)((ntiles + 127) / 128), 128, 0, st>>>(tiles, nt);
+  SPB_LAUNCH_CHECK();
+  dim3 tb(32, 8), tg((m + 31) / 32, (unsigned)((ldk + 31) / 32));
+  split_transpose_kernel<<<tg, tb, 0, st>>>(Y, n, m, sd, H, L, (int)ldk);
+  SPB_LAUNCH_CHECK();
+  CUtensorMap mH = make_map(H, m, (int)ldk, (int)ldk), mL = make_map(L, m, (int)ldk, (int)ldk);
+  const size_t smem = (size_t)STAGES * STAGE_BYTES + 1024;
+  SPB_CUDA(cudaFuncSetAttribute(gram_tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  gram_tile_kernel<<<(unsigned)ntiles, 128, smem, st>>>(mH, mL, tiles, m, (int)(ldk / BK), G, err);
+  SPB_LAUNCH_CHECK();
+  symmetrize_kernel<<<(unsigned)(((size_t)m * m + 255) / 256), 256, 0, st>>>(G, m, S);
+  SPB_LAUNCH_CHECK();
+  int h = 0;
+  SPB_CUDA(cudaMemcpyAsync(&h, err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  SPB_CUDA(cudaStreamSynchronize(st));
+  if (h) fail(SYMPROP_ERR_TIMEOUT, "tensor-core Gram: a bounded wait expired");
+}
+
 }  // namespace gram
 }  // namespace spb
+
+// See include/symprop.h: allocation-free tensor-core Gram.
+extern "C" int symprop_gram_device_noalloc(const float *dY, uint64_t n, uint32_t m, const float *dscale,
+                                           double *dG, void *stream) {
+  return spb::guard([&] {
+    if (!dY || !dscale || !dG) spb::fail(SYMPROP_ERR_INVALID, "null argument");
+    if (n == 0 || m == 0 || n >= (1ull << 31)) spb::fail(SYMPROP_ERR_INVALID, "bad sizes");
+    spb::gram::gram_split_bf16_noalloc((cudaStream_t)stream, dY, (int)n, (int)m, dscale, dG);
+  });
+}

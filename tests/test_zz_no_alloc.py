@@ -1,0 +1,49 @@
+"""GPU test of the allocation-free Gram entry point
+(symprop_gram_device_noalloc), for callers that cannot allocate device
+memory at call time.  It must give the same matrix as the regular
+tensor-core entry point (symprop_gram_device, FP32 input) on two calls in a
+row (the fixed workspace keeps the previous call's contents), and reject
+inputs whose workspace does not fit its fixed array.  The file sorts last so
+that a run stopping at the first failure has run everything else first; it
+also passes alone in a fresh process."""
+import ctypes
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+P = ctypes.c_void_p
+
+
+def test_noalloc_gram_matches_regular_entry_point_twice(gpu):
+    import torch
+    L = gpu.lib()
+    for (n, m, seed) in [(3000, 330, 1), (5000, 130, 2)]:
+        g = torch.Generator(device="cpu").manual_seed(seed)
+        Y = (torch.randn(n, m, generator=g) * 2.0).float().cuda()
+        sd = (torch.rand(m, generator=g) + 0.5).float().cuda()
+        G_ref = torch.empty(m, m, dtype=torch.float64, device="cuda")
+        assert L.symprop_gram_device(P(Y.data_ptr()), n, m, P(sd.data_ptr()), P(G_ref.data_ptr()),
+                                     gpu.FP32, None) == 0
+        for _ in range(2):
+            G = torch.full((m, m), float("nan"), dtype=torch.float64, device="cuda")
+            st = L.symprop_gram_device_noalloc(P(Y.data_ptr()), n, m, P(sd.data_ptr()),
+                                               P(G.data_ptr()), None)
+            assert st == 0, L.symprop_last_error()
+            torch.cuda.synchronize()
+            err = ((G - G_ref).norm() / G_ref.norm()).item()
+            # same kernels on the same inputs; the bound is the one the dense
+            # tests use between the tensor-core path and its emulation
+            assert err <= 2e-4, err
+            assert torch.equal(G, G.T)
+
+
+def test_noalloc_rejects_oversized_workspace(gpu):
+    import torch
+    L = gpu.lib()
+    n, m = 200000, 816  # about 650 MB of split operands
+    Y = torch.zeros(1, dtype=torch.float32, device="cuda")
+    G = torch.zeros(1, dtype=torch.float64, device="cuda")
+    st = L.symprop_gram_device_noalloc(P(Y.data_ptr()), n, m, P(Y.data_ptr()), P(G.data_ptr()), None)
+    assert st == gpu.ERR_SIZE
+    assert b"fixed array" in L.symprop_last_error()
