@@ -59,9 +59,8 @@ struct WarpParams {
   uint32_t ndesc, desc_begin[kMaxL + 1], desc_count[kMaxL + 1];
   uint32_t m[kMaxL + 1], m4[kMaxL + 1];
   uint32_t pair_src[kMaxL * kMaxL];  // level N-3 tensor of the positions other than {k,t}
-  const int2 *tiles;                 // (first row, first column) per tile
-  const uint4 *rowdesc;              // per tile: (rp << 8) | jp of its 4 rows
-  const uint4 *rowoff;               // per tile: lex offset - jp of its 4 rows, or kPadRow
+  const int4 *tiles;                 // per tile: (first row r0 inside block j, j, first column x0, 0)
+  const uint4 *rowoff;               // per tile: lex offset - j of its 4 rows, or kPadRow
   uint32_t ntiles;
   uint32_t wsz;                      // per-warp staging elements: 2*L*R4 + ksz4
 };
@@ -112,22 +111,15 @@ __global__ void __launch_bounds__(kThreads, min_blocks<T>()) s3ttmc_warp_kernel(
   if (!heavy && item >= p.nchunks) return;  // light CTAs have no barrier below
   const Chunk ch = p.chunks[item];
 
-  // this lane's tiles and their row descriptors
-  int2 tl[NTL];
-  uint32_t rp[NTL][4], jp[NTL][4];
+  // this lane's tiles: 4 consecutive rows r0..r0+3 of block j (all with last
+  // index j) times columns x0..x0+3
+  int4 tl[NTL];
   bool live[NTL];
 #pragma unroll
   for (int i = 0; i < NTL; ++i) {
     const uint32_t id = (uint32_t)lane + 32u * i;
     live[i] = id < p.ntiles;
-    tl[i] = live[i] ? p.tiles[id] : make_int2(0, 0);
-    const uint4 d = live[i] ? p.rowdesc[id] : make_uint4(0, 0, 0, 0);
-    const uint32_t dd[4] = {d.x, d.y, d.z, d.w};
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      rp[i][q] = dd[q] >> 8;
-      jp[i][q] = dd[q] & 0xffu;
-    }
+    tl[i] = live[i] ? p.tiles[id] : make_int4(0, 0, 0, 0);
   }
 
   T acc[NTL][4][4], cmp[NTL][4][4], tmp[NTL][4][4];
@@ -185,51 +177,55 @@ __global__ void __launch_bounds__(kThreads, min_blocks<T>()) s3ttmc_warp_kernel(
         __syncwarp();
       }
     }
-    // last level
+    // last level: the parents K(S \ s_k) at rows (r0+q, j) are
+    //   sum_{t != k} K(S \ {s_k, s_t})[r0+q] * U[s_t][j]
+    // (level N-3 tensors, or U rows for order 4), then the tile gets
+    // sum_k A_k[q] * (c U[s_k])[x0 + cc]
 #pragma unroll
     for (int i = 0; i < NTL; ++i) {
       if (!live[i]) continue;
-      T w[L][4];
+      const uint32_t r0 = (uint32_t)tl[i].x, jt = (uint32_t)tl[i].y, x0 = (uint32_t)tl[i].z;
+      T w[L][4], uj[L], A[L][4];
 #pragma unroll
-      for (int k = 0; k < L; ++k) ld4(sW + k * R4 + tl[i].y, w[k]);
+      for (int k = 0; k < L; ++k) ld4(sW + k * R4 + x0, w[k]);
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        T uj[L], A[L];
+      for (int t = 0; t < L; ++t) uj[t] = sU[t * R4 + jt];
+      if constexpr (L == 2) {
 #pragma unroll
-        for (int t = 0; t < L; ++t) uj[t] = sU[t * R4 + jp[i][q]];
-        if constexpr (L == 2) {
-          A[0] = uj[1];
-          A[1] = uj[0];
-        } else {
-          T kp[L * L];
-#pragma unroll
-          for (int k = 0; k < L; ++k)
-#pragma unroll
-            for (int t = k + 1; t < L; ++t) {
-              const uint32_t s = p.pair_src[pidx(k, t, L)];
-              if constexpr (L == 3) kp[pidx(k, t, L)] = sU[(s & 0xffu) * R4 + rp[i][q]];
-              else kp[pidx(k, t, L)] = sK[s + rp[i][q]];
-            }
-#pragma unroll
-          for (int k = 0; k < L; ++k) {
-            T a = T(0);
-#pragma unroll
-            for (int t = 0; t < L; ++t) {
-              if (t == k) continue;
-              a += kp[k < t ? pidx(k, t, L) : pidx(t, k, L)] * uj[t];
-            }
-            A[k] = a;
-          }
+        for (int q = 0; q < 4; ++q) {
+          A[0][q] = q == 0 ? uj[1] : T(0);
+          A[1][q] = q == 0 ? uj[0] : T(0);
         }
+      } else {
+#pragma unroll
+        for (int k = 0; k < L; ++k)
+#pragma unroll
+          for (int q = 0; q < 4; ++q) A[k][q] = T(0);
+#pragma unroll
+        for (int k = 0; k < L; ++k)
+#pragma unroll
+          for (int t = k + 1; t < L; ++t) {
+            const uint32_t s = p.pair_src[pidx(k, t, L)];
+            T kv[4];
+            if constexpr (L == 3) ld4(sU + (s & 0xffu) * R4 + r0, kv);
+            else ld4(sK + s + r0, kv);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+              A[k][q] += kv[q] * uj[t];
+              A[t][q] += kv[q] * uj[k];
+            }
+          }
+      }
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
 #pragma unroll
         for (int cc = 0; cc < 4; ++cc) {
           T s = T(0);
 #pragma unroll
-          for (int k = 0; k < L; ++k) s += A[k] * w[k][cc];
+          for (int k = 0; k < L; ++k) s += A[k][q] * w[k][cc];
           if constexpr (kExact) acc[i][q][cc] += s;
           else tmp[i][q][cc] += s;
         }
-      }
     }
     if constexpr (!kExact) {
       if (++pending == 4) {
@@ -277,9 +273,9 @@ __global__ void __launch_bounds__(kThreads, min_blocks<T>()) s3ttmc_warp_kernel(
         if (rof[q] == kPadRow) continue;
 #pragma unroll
         for (int cc = 0; cc < 4; ++cc) {
-          const uint32_t j = (uint32_t)tl[i].y + cc;
-          if (j >= R || j < jp[i][q]) continue;
-          const uint32_t qo = rof[q] + j;
+          const uint32_t x = (uint32_t)tl[i].z + cc;
+          if (x >= R || x < (uint32_t)tl[i].y) continue;
+          const uint32_t qo = rof[q] + x;
           if (ch.slot == kDirect) Yrow[qo] = acc[i][q][cc];
           else Prow[qo] = (double)acc[i][q][cc];
         }
@@ -302,17 +298,16 @@ __global__ void __launch_bounds__(kThreads, min_blocks<T>()) s3ttmc_warp_kernel(
   __syncthreads();
   for (uint32_t e = tid; e < p.ntiles * 16; e += kThreads) {
     const uint32_t tile = e >> 4, q = (e >> 2) & 3, cc = e & 3;
-    const uint32_t j = (uint32_t)p.tiles[tile].y + cc;
+    const int4 tt = p.tiles[tile];
+    const uint32_t x = (uint32_t)tt.z + cc;
     const uint4 ro = p.rowoff[tile];
-    const uint4 rd = p.rowdesc[tile];
     const uint32_t rof = q == 0 ? ro.x : q == 1 ? ro.y : q == 2 ? ro.z : ro.w;
-    const uint32_t jq = (q == 0 ? rd.x : q == 1 ? rd.y : q == 2 ? rd.z : rd.w) & 0xffu;
-    if (rof == kPadRow || j >= R || j < jq) continue;
+    if (rof == kPadRow || x >= R || x < (uint32_t)tt.y) continue;
     T s = T(0);
 #pragma unroll
     for (int w2 = 0; w2 < kWarps; ++w2) s += red[((size_t)w2 * p.ntiles + tile) * 16 + (e & 15)];
-    if (ch.slot == kDirect) Yrow[rof + j] = s;
-    else Prow[rof + j] = (double)s;
+    if (ch.slot == kDirect) Yrow[rof + x] = s;
+    else Prow[rof + x] = (double)s;
   }
 }
 
@@ -328,8 +323,8 @@ struct WarpPlan {
   DBuf<WDesc> desc;
   uint32_t ndesc = 0, desc_begin[kMaxL + 1] = {}, desc_count[kMaxL + 1] = {};
   uint32_t pair_src[kMaxL * kMaxL] = {};
-  DBuf<int2> tiles;
-  DBuf<uint4> rowdesc, rowoff;
+  DBuf<int4> tiles;
+  DBuf<uint4> rowoff;
   uint32_t ntiles = 0, ksz4 = 0, wsz = 0;
   size_t smem[2] = {0, 0};
 };
@@ -349,19 +344,10 @@ std::shared_ptr<WarpPlan> warp_plan(uint32_t N, uint32_t R) {
   std::vector<uint32_t> starts((size_t)(L + 1) * (R + 1), 0);
   for (uint32_t d = 1; d <= L; ++d)
     for (uint32_t j = 0; j <= R; ++j) starts[(size_t)d * (R + 1) + j] = (uint32_t)symsize(j, d);
-  // tiles of the last level: rows = colex rank of the prefix (order L-1)
-  std::vector<int2> tiles;
-  const uint32_t *stL = &starts[(size_t)L * (R + 1)];
-  for (uint32_t j0 = 0; j0 < pl->R4; j0 += 4) {
-    uint32_t jl = std::min(j0 + 3, R - 1);
-    uint32_t cnt = stL[jl + 1] - stL[jl];
-    for (uint32_t r0 = 0; r0 < cnt; r0 += 4) tiles.push_back(make_int2((int)r0, (int)j0));
-  }
-  pl->ntiles = (uint32_t)tiles.size();
-  pl->NTL = (pl->ntiles + 31) / 32;
-  if (pl->NTL > (uint32_t)kMaxNTL) return pl;
-  // per prefix row r (colex, order L-1): jp = its last id, rp = colex rank of
-  // the prefix without it, off = lex index of (prefix, jp) - jp
+  // tiles of the last level, aligned to the colex blocks of the prefixes: a
+  // tile is rows r0..r0+3 of block j (prefixes of order L-1 whose last id is
+  // j, taken in colex order of the rest) times columns x0..x0+3, x0 from
+  // the column block holding j
   auto colex = [](const std::vector<uint32_t> &q) {
     uint64_t cx = 0;
     for (size_t i = 0; i < q.size(); ++i) cx += symsize(q[i], i + 1);
@@ -369,33 +355,30 @@ std::shared_ptr<WarpPlan> warp_plan(uint32_t N, uint32_t R) {
   };
   std::vector<uint32_t> lexL(pl->m[L]);
   for_each_sorted(R, (int)L, [&](const std::vector<uint32_t> &q, uint64_t lin) { lexL[colex(q)] = (uint32_t)lin; });
-  std::vector<uint32_t> row_rp(pl->m[L - 1]), row_jp(pl->m[L - 1]), row_off(pl->m[L - 1]);
+  // row_off[prefix colex rank] = lex index of (prefix, last) - last
+  std::vector<uint32_t> row_off(pl->m[L - 1]);
   for_each_sorted(R, (int)(L - 1), [&](const std::vector<uint32_t> &q, uint64_t) {
-    const uint32_t r = (uint32_t)colex(q);
-    const uint32_t j = q.back();
-    std::vector<uint32_t> pre(q.begin(), q.end() - 1);
-    row_rp[r] = (uint32_t)colex(pre);
-    row_jp[r] = j;
     std::vector<uint32_t> full = q;
-    full.push_back(j);
-    row_off[r] = lexL[colex(full)] - j;
+    full.push_back(q.back());
+    row_off[colex(q)] = lexL[colex(full)] - q.back();
   });
-  std::vector<uint4> rdesc(pl->ntiles), roff(pl->ntiles);
-  for (uint32_t t = 0; t < pl->ntiles; ++t) {
-    uint32_t d[4], o[4];
-    for (int q = 0; q < 4; ++q) {
-      uint32_t r = (uint32_t)tiles[t].x + q;
-      if (r < pl->m[L - 1]) {
-        d[q] = (row_rp[r] << 8) | row_jp[r];
-        o[q] = row_off[r];
-      } else {  // padding row: evaluated at a safe index, never written
-        d[q] = 0;
-        o[q] = kPadRow;
+  const uint32_t *stP = &starts[(size_t)(L - 1) * (R + 1)];
+  std::vector<int4> tiles;
+  std::vector<uint4> roff;
+  for (uint32_t j = 0; j < R; ++j) {
+    const uint32_t base = stP[j], cnt = stP[j + 1] - stP[j];
+    for (uint32_t r0 = 0; r0 < cnt; r0 += 4) {
+      uint32_t o[4];
+      for (uint32_t q = 0; q < 4; ++q) o[q] = (r0 + q < cnt) ? row_off[base + r0 + q] : kPadRow;
+      for (uint32_t x0 = j / 4 * 4; x0 < pl->R4; x0 += 4) {
+        tiles.push_back(make_int4((int)r0, (int)j, (int)x0, 0));
+        roff.push_back(make_uint4(o[0], o[1], o[2], o[3]));
       }
     }
-    rdesc[t] = make_uint4(d[0], d[1], d[2], d[3]);
-    roff[t] = make_uint4(o[0], o[1], o[2], o[3]);
   }
+  pl->ntiles = (uint32_t)tiles.size();
+  pl->NTL = (pl->ntiles + 31) / 32;
+  if (pl->NTL > (uint32_t)kMaxNTL) return pl;
   // jtab and descriptors for levels 2..L-2
   std::vector<uint8_t> jt;
   for (uint32_t d = 2; d + 2 <= L; ++d) {
@@ -454,9 +437,7 @@ std::shared_ptr<WarpPlan> warp_plan(uint32_t N, uint32_t R) {
   if (!desc.empty())
     SPB_CUDA(cudaMemcpy(pl->desc.p, desc.data(), desc.size() * sizeof(WDesc), cudaMemcpyHostToDevice));
   pl->tiles.alloc(tiles.size());
-  SPB_CUDA(cudaMemcpy(pl->tiles.p, tiles.data(), tiles.size() * sizeof(int2), cudaMemcpyHostToDevice));
-  pl->rowdesc.alloc(rdesc.size());
-  SPB_CUDA(cudaMemcpy(pl->rowdesc.p, rdesc.data(), rdesc.size() * sizeof(uint4), cudaMemcpyHostToDevice));
+  SPB_CUDA(cudaMemcpy(pl->tiles.p, tiles.data(), tiles.size() * sizeof(int4), cudaMemcpyHostToDevice));
   pl->rowoff.alloc(roff.size());
   SPB_CUDA(cudaMemcpy(pl->rowoff.p, roff.data(), roff.size() * sizeof(uint4), cudaMemcpyHostToDevice));
   pl->ok = true;
@@ -528,7 +509,6 @@ void warp_launch(const WarpPlan &pl, const TensorState &t, const void *dU, void 
   }
   for (int i = 0; i < kMaxL * kMaxL; ++i) wp.pair_src[i] = pl.pair_src[i];
   wp.tiles = pl.tiles.p;
-  wp.rowdesc = pl.rowdesc.p;
   wp.rowoff = pl.rowoff.p;
   wp.ntiles = pl.ntiles;
   wp.wsz = pl.wsz;
