@@ -8,6 +8,8 @@
 // becomes CholQR2 with a Householder QR fallback.
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <vector>
 
 #include "dense.cuh"
@@ -315,8 +317,9 @@ __global__ void __launch_bounds__(1024) jacobi_kernel(const double *S, int n, do
                                                       double *V_out) {
   extern __shared__ double sm[];
   const int np = (n + 1) & ~1;
-  double *A = sm;            // np x np
-  double *V = sm + np * np;  // np x np
+  const int ld = np + 1;     // odd row stride: column sweeps hit distinct banks
+  double *A = sm;            // np x ld
+  double *V = sm + np * ld;  // np x ld
   __shared__ double cs[2 * 64];
   __shared__ int pr[2 * 64];
   __shared__ int order[128];
@@ -324,19 +327,22 @@ __global__ void __launch_bounds__(1024) jacobi_kernel(const double *S, int n, do
   const int tid = threadIdx.x, nt = blockDim.x;
   for (int idx = tid; idx < np * np; idx += nt) {
     int i = idx / np, j = idx % np;
-    A[idx] = (i < n && j < n) ? S[i * n + j] : 0.0;
-    V[idx] = (i == j) ? 1.0 : 0.0;
+    A[i * ld + j] = (i < n && j < n) ? S[i * n + j] : 0.0;
+    V[i * ld + j] = (i == j) ? 1.0 : 0.0;
   }
   __syncthreads();
   double fro = 0;
-  for (int idx = tid; idx < np * np; idx += nt) fro += A[idx] * A[idx];
+  for (int idx = tid; idx < np * np; idx += nt) {
+    const double x = A[(idx / np) * ld + idx % np];
+    fro += x * x;
+  }
   fro = block_sum(fro, red);
   const int half = np / 2;
   for (int sweep = 0; sweep < 60 && np > 1; ++sweep) {
     double off = 0;
     for (int idx = tid; idx < np * np; idx += nt) {
       int i = idx / np, j = idx % np;
-      if (i != j) off += A[idx] * A[idx];
+      if (i != j) off += A[i * ld + j] * A[i * ld + j];
     }
     off = block_sum(off, red);
     if (!(off > 1e-30 * fro)) break;
@@ -349,10 +355,10 @@ __global__ void __launch_bounds__(1024) jacobi_kernel(const double *S, int n, do
         int p = min(a, b), q = max(a, b);
         pr[2 * k] = p;
         pr[2 * k + 1] = q;
-        double apq = A[p * np + q];
+        double apq = A[p * ld + q];
         double c = 1.0, s = 0.0;
         if (apq != 0.0) {
-          double tau = (A[q * np + q] - A[p * np + p]) / (2.0 * apq);
+          double tau = (A[q * ld + q] - A[p * ld + p]) / (2.0 * apq);
           double t = (tau >= 0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
           c = 1.0 / sqrt(1.0 + t * t);
           s = t * c;
@@ -365,21 +371,21 @@ __global__ void __launch_bounds__(1024) jacobi_kernel(const double *S, int n, do
         int k = idx / np, col = idx % np;
         int p = pr[2 * k], q = pr[2 * k + 1];
         double c = cs[2 * k], s = cs[2 * k + 1];
-        double a = A[p * np + col], b = A[q * np + col];
-        A[p * np + col] = c * a - s * b;
-        A[q * np + col] = s * a + c * b;
+        double a = A[p * ld + col], b = A[q * ld + col];
+        A[p * ld + col] = c * a - s * b;
+        A[q * ld + col] = s * a + c * b;
       }
       __syncthreads();
       for (int idx = tid; idx < half * np; idx += nt) {  // cols: A <- A J, V <- V J
         int k = idx / np, row = idx % np;
         int p = pr[2 * k], q = pr[2 * k + 1];
         double c = cs[2 * k], s = cs[2 * k + 1];
-        double a = A[row * np + p], b = A[row * np + q];
-        A[row * np + p] = c * a - s * b;
-        A[row * np + q] = s * a + c * b;
-        double va = V[row * np + p], vb = V[row * np + q];
-        V[row * np + p] = c * va - s * vb;
-        V[row * np + q] = s * va + c * vb;
+        double a = A[row * ld + p], b = A[row * ld + q];
+        A[row * ld + p] = c * a - s * b;
+        A[row * ld + q] = s * a + c * b;
+        double va = V[row * ld + p], vb = V[row * ld + q];
+        V[row * ld + p] = c * va - s * vb;
+        V[row * ld + q] = s * va + c * vb;
       }
       __syncthreads();
     }
@@ -389,17 +395,17 @@ __global__ void __launch_bounds__(1024) jacobi_kernel(const double *S, int n, do
     for (int i = 0; i < n; ++i) order[i] = i;
     for (int i = 0; i < n; ++i)
       for (int j = i + 1; j < n; ++j)
-        if (A[order[j] * np + order[j]] > A[order[i] * np + order[i]]) {
+        if (A[order[j] * ld + order[j]] > A[order[i] * ld + order[i]]) {
           int t = order[i];
           order[i] = order[j];
           order[j] = t;
         }
   }
   __syncthreads();
-  for (int i = tid; i < n; i += nt) w_out[i] = A[order[i] * np + order[i]];
+  for (int i = tid; i < n; i += nt) w_out[i] = A[order[i] * ld + order[i]];
   for (int idx = tid; idx < n * n; idx += nt) {
     int row = idx / n, k = idx % n;
-    V_out[idx] = V[row * np + order[k]];
+    V_out[idx] = V[row * ld + order[k]];
   }
 }
 
@@ -595,7 +601,7 @@ static void project_out(cudaStream_t st, const double *Q, int ldq, int width, do
 void jacobi_eig(cudaStream_t st, const double *S, int n, double *w, double *V) {
   if (n > kJacobiMax) fail(SYMPROP_ERR_SIZE, "jacobi_eig: n=%d > %d", n, kJacobiMax);
   int np = (n + 1) & ~1;
-  size_t smem = 2 * sizeof(double) * np * np;
+  size_t smem = 2 * sizeof(double) * np * (np + 1);
   SPB_CUDA(cudaFuncSetAttribute(jacobi_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   jacobi_kernel<<<1, 1024, smem, st>>>(S, n, w, V);
   SPB_LAUNCH_CHECK();
@@ -618,6 +624,15 @@ template <typename Ts, typename Td> void convert(cudaStream_t st, const Ts *src,
 }
 template void convert<double, float>(cudaStream_t, const double *, float *, size_t);
 template void convert<float, double>(cudaStream_t, const float *, double *, size_t);
+
+// SPB_TRACE_EIG=1 prints the restart count and final residual of each solve
+static bool eig_trace() {
+  static const bool on = [] {
+    const char *e = std::getenv("SPB_TRACE_EIG");
+    return e && *e && *e != '0';
+  }();
+  return on;
+}
 
 // Block Krylov (block Lanczos with full re-orthogonalisation and thick
 // restart) for the top-r eigenpairs of S.  Projected problems of at most
@@ -698,6 +713,9 @@ int top_eigs(cudaStream_t st, const double *S, int s, int r, double *V, double *
     double worst = 0;
     for (int i = 0; i < r; ++i) worst = std::max(worst, hres[i] / scale);
     if (worst <= tol || it == max_restarts) {
+      if (eig_trace())
+        std::fprintf(stderr, "top_eigs: s=%d r=%d b=%d restarts=%d residual=%.3e tol=%.1e\n", s, r, b, it,
+                     worst, tol);
       copy_cols_kernel<<<cdiv((long long)s * r, 256), 256, 0, st>>>(X.as<double>(), b, s, r, V, r);
       SPB_LAUNCH_CHECK();
       for (int i = 0; i < r; ++i) lam[i] = hw[i];

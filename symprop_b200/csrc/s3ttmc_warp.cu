@@ -1,29 +1,31 @@
-// S3TTMc, warp-per-owner schedule (default when the packed output fits in
-// the registers of one warp: up to 4 output tiles of 4 x 4 per lane, e.g.
-// order 4 / R <= 16, order 5 / R <= 10, order 6 / R <= 8).
+// S3TTMc, warp-per-owner schedule (the default for orders 3..5 when the
+// staged U rows fit two values per lane, e.g. order 4 / R <= 16, order 5 /
+// R <= 16).
 //
 // Same mathematics as the reference's level sweep
 // (CompressedDTree::kronecker_product_opt5, src/compressed_dtree.cpp:421-518;
 // SymOuterProd, include/detail/dense/symtensor.hpp:24-39):
 //     Y[i] += c * K(S),  K(S) = sum_k K(S \ s_k) (x) U[s_k].
-// A warp streams owners (tree leaves) of one row, one leaf per step, with no
-// CTA barrier inside the loop:
+// A warp streams the owners (tree leaves) of one work item, one leaf per
+// step, with no CTA barrier inside the loop:
 //   * lanes stage the leaf's N-1 U rows (and c * U rows) in warp-private
-//     shared memory;
+//     shared memory; the rows of the next leaf are loaded while the current
+//     one is computed;
 //   * levels 2..N-3 of the recursion are built in warp-private shared memory
 //     (colexicographic order, see s3ttmc_tiled.cu);
 //   * the last level is never stored: for each of its 4 x 4 output tiles a
 //     lane evaluates the N-1 parent tensors K(S \ s_k) at the tile's 4 rows
 //     from level N-3 and U in registers, then adds the rank-(N-1) product
 //     with the c * U rows.
-// Work items (a row, or a slice of a long row) with at most kLightOwners
-// owners take one warp each and are written straight from registers; larger
-// ones take the 4 warps of a CTA, whose tiles are added in warp order
-// (deterministic).  For a fixed prefix p the outputs (p, x), x >= last(p),
-// are consecutive in the reference's lexicographic packed order, so a tile
-// row is written at a precomputed row offset + x (no permutation table).
-// FP32 mode folds the lane's plain FP32 sums into a Kahan-compensated
-// accumulator every 4 owners.
+// The output tiles of a row are split over G warps (NTL tiles per lane), so
+// the accumulators stay in registers whatever the packed row length; each of
+// the G warps streams the same owners.  A work item is a row, or a slice of
+// at most 256 owners of a long row whose FP64 partial sums a second kernel
+// adds in a fixed order.  For a fixed prefix p the outputs (p, x),
+// x >= last(p), are consecutive in the reference's lexicographic packed
+// order, so a tile row is written at a precomputed row offset + x (no
+// permutation table).  FP32 mode folds the lane's plain FP32 sums into a
+// Kahan-compensated accumulator in shared memory every 8 owners.
 #include <algorithm>
 
 #include "s3ttmc_warp.cuh"
@@ -32,6 +34,7 @@ namespace spb {
 namespace {
 
 constexpr int kWarps = 4, kThreads = kWarps * 32, kMaxL = 7, kMaxNTL = 4;
+constexpr int kFold = 8;  // FP32: owners summed plainly between Kahan folds
 constexpr uint32_t kURow = 0x80000000u;
 constexpr uint32_t kPadRow = 0xffffffffu;
 
@@ -42,7 +45,7 @@ struct WDesc {
 
 struct WarpParams {
   const Chunk *chunks;
-  uint32_t nchunks, nheavy;
+  uint32_t nchunks;
   const uint32_t *own_S;
   const void *own_c;
   uint32_t sstride;
@@ -77,58 +80,237 @@ template <typename T> __device__ __forceinline__ void ld4(const T *p, T (&v)[4])
 
 __host__ __device__ constexpr int pidx(int k, int t, int L) { return k * L + t; }  // k < t
 
-template <typename T> constexpr int min_blocks() { return sizeof(T) == 8 ? 3 : 2; }
+// CTAs per SM the register budget is sized for (accumulators: NTL x 16
+// values per lane)
+template <typename T, int NTL> __host__ __device__ constexpr int min_blocks() {
+  return sizeof(T) == 8 ? (NTL == 1 ? 4 : NTL <= 3 ? 3 : 2) : (NTL <= 3 ? 4 : 3);
+}
 
+// U values of one owner staged per lane by the warp kernel (the plan checks
+// L * R4 <= 32 * kP)
+template <int L> __host__ __device__ constexpr int stage_per_lane() { return L <= 2 ? 4 : 2; }
+
+// Shared tables of the levels 2..L-2 recursion (copied once per CTA).
+struct SmemTables {
+  uint32_t *start;
+  uint8_t *jt;
+  WDesc *desc;
+  unsigned char *rest;  // first byte after the tables (16-byte aligned)
+};
+
+template <int L>
+__device__ __forceinline__ SmemTables load_tables(const WarpParams &p, unsigned char *smem, int tid, int nthr) {
+  SmemTables tb;
+  size_t off = 0;
+  tb.start = reinterpret_cast<uint32_t *>(smem + off);
+  off += (((size_t)(L + 1) * (p.R + 1) * 4) + 15) / 16 * 16;
+  tb.jt = smem + off;
+  off += ((size_t)p.jtab_len + 15) / 16 * 16;
+  tb.desc = reinterpret_cast<WDesc *>(smem + off);
+  off += ((size_t)p.ndesc * sizeof(WDesc) + 15) / 16 * 16;
+  tb.rest = smem + off;
+  if constexpr (L >= 4) {
+    for (uint32_t i = tid; i < (uint32_t)(L + 1) * (p.R + 1); i += nthr) tb.start[i] = p.starts[i];
+    for (uint32_t i = tid; i < p.jtab_len; i += nthr) tb.jt[i] = p.jtab[i];
+    const uint32_t *src = reinterpret_cast<const uint32_t *>(p.desc);
+    uint32_t *dst = reinterpret_cast<uint32_t *>(tb.desc);
+    const uint32_t words = p.ndesc * (uint32_t)(sizeof(WDesc) / 4);
+    for (uint32_t i = tid; i < words; i += nthr) dst[i] = src[i];
+  }
+  return tb;
+}
+
+// One level d (2 <= d <= L-2) of the recursion for one owner: every
+// sub-multiset tensor of order d, colex order, from level d-1 (or U rows)
+// times U; elements strided over nthr threads.
+template <int L, typename T>
+__device__ __forceinline__ void dp_level(const WarpParams &p, const SmemTables &tb, int d, const T *sU, T *sK,
+                                         uint32_t tid, uint32_t nthr) {
+  const uint32_t R4 = p.R4;
+  const uint32_t md = p.m[d], md4 = p.m4[d], nd = p.desc_count[d];
+  const uint8_t *jt = tb.jt + p.jtab_off[d];
+  const uint32_t *stt = tb.start + d * (p.R + 1);
+  const WDesc *dd = tb.desc + p.desc_begin[d];
+  for (uint32_t it = tid; it < nd * md4; it += nthr) {
+    const uint32_t mi = it / md4, e = it - mi * md4;
+    T v = T(0);
+    if (e < md) {
+      const uint32_t j = jt[e], r = e - stt[j];
+      const WDesc &ds = dd[mi];
+#pragma unroll
+      for (int t = 0; t < kMaxL; ++t) {
+        if (t >= d) break;
+        const uint32_t s = ds.src[t];
+        const T a = (s & kURow) ? sU[(s & 0xffu) * R4 + r] : sK[s + r];
+        v += a * sU[ds.k[t] * R4 + j];
+      }
+    }
+    sK[dd[mi].dst + e] = v;
+  }
+}
+
+// The last level for one owner on this thread's tiles: the parents
+// K(S \ s_k) at rows (r0+q, j) are
+//   sum_{t != k} K(S \ {s_k, s_t})[r0+q] * U[s_t][j]
+// (level N-3 tensors, or U rows for order 4), then the tile gets
+// sum_k A_k[q] * (c U[s_k])[x0 + cc].
 template <int L, int NTL, typename T>
-__global__ void __launch_bounds__(kThreads, min_blocks<T>()) s3ttmc_warp_kernel(const WarpParams p) {
+__device__ __forceinline__ void tile_step(const WarpParams &p, const T *sU, const T *sW, const T *sK,
+                                          const int4 (&tl)[NTL], const bool (&live)[NTL], T (&acc)[NTL][4][4]) {
+  const uint32_t R4 = p.R4;
+#pragma unroll
+  for (int i = 0; i < NTL; ++i) {
+    if (!live[i]) continue;
+    const uint32_t r0 = (uint32_t)tl[i].x, jt = (uint32_t)tl[i].y, x0 = (uint32_t)tl[i].z;
+    T w[L][4], uj[L], A[L][4];
+#pragma unroll
+    for (int k = 0; k < L; ++k) ld4(sW + k * R4 + x0, w[k]);
+#pragma unroll
+    for (int t = 0; t < L; ++t) uj[t] = sU[t * R4 + jt];
+    if constexpr (L == 2) {
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        A[0][q] = q == 0 ? uj[1] : T(0);
+        A[1][q] = q == 0 ? uj[0] : T(0);
+      }
+    } else {
+#pragma unroll
+      for (int k = 0; k < L; ++k)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) A[k][q] = T(0);
+#pragma unroll
+      for (int k = 0; k < L; ++k)
+#pragma unroll
+        for (int t = k + 1; t < L; ++t) {
+          const uint32_t s = p.pair_src[pidx(k, t, L)];
+          T kv[4];
+          if constexpr (L == 3) ld4(sU + (s & 0xffu) * R4 + r0, kv);
+          else ld4(sK + s + r0, kv);
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            A[k][q] += kv[q] * uj[t];
+            A[t][q] += kv[q] * uj[k];
+          }
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+#pragma unroll
+      for (int cc = 0; cc < 4; ++cc) {
+        T s = acc[i][q][cc];
+#pragma unroll
+        for (int k = 0; k < L; ++k) s += A[k][q] * w[k][cc];
+        acc[i][q][cc] = s;
+      }
+  }
+}
+
+// FP32: fold the plain sums into the thread's Kahan pairs (sum,
+// compensation) kept in shared memory at slot e * stride + me.
+template <int NTL, typename T>
+__device__ __forceinline__ void kahan_fold(float2 *sK2, uint32_t stride, uint32_t me, T (&acc)[NTL][4][4]) {
+#pragma unroll
+  for (int i = 0; i < NTL; ++i)
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+#pragma unroll
+      for (int cc = 0; cc < 4; ++cc) {
+        float2 &ks = sK2[((i * 4 + q) * 4 + cc) * stride + me];
+        float2 k = ks;
+        const float y = (float)acc[i][q][cc] - k.y;
+        const float s2 = k.x + y;
+        k.y = (s2 - k.x) - y;
+        k.x = s2;
+        ks = k;
+        acc[i][q][cc] = T(0);
+      }
+}
+
+template <int NTL, typename T>
+__device__ __forceinline__ void kahan_result(const float2 *sK2, uint32_t stride, uint32_t me, T (&acc)[NTL][4][4]) {
+#pragma unroll
+  for (int i = 0; i < NTL; ++i)
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+#pragma unroll
+      for (int cc = 0; cc < 4; ++cc) {
+        const float2 k = sK2[((i * 4 + q) * 4 + cc) * stride + me];
+        acc[i][q][cc] = (T)(k.x - k.y);
+      }
+}
+
+// Write this thread's tiles: lex index = row offset + column.
+template <int NTL, typename T>
+__device__ __forceinline__ void write_tiles(const WarpParams &p, const Chunk &ch, const int4 (&tl)[NTL],
+                                            const bool (&live)[NTL], const uint32_t (&ids)[NTL],
+                                            const T (&acc)[NTL][4][4]) {
+  T *Yrow = reinterpret_cast<T *>(p.Y) + (uint64_t)ch.row * p.ldy;
+  double *Prow = p.partials + (uint64_t)ch.slot * p.mL;
+#pragma unroll
+  for (int i = 0; i < NTL; ++i) {
+    if (!live[i]) continue;
+    const uint4 ro = p.rowoff[ids[i]];
+    const uint32_t rof[4] = {ro.x, ro.y, ro.z, ro.w};
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      if (rof[q] == kPadRow) continue;
+#pragma unroll
+      for (int cc = 0; cc < 4; ++cc) {
+        const uint32_t x = (uint32_t)tl[i].z + cc;
+        if (x >= p.R || x < (uint32_t)tl[i].y) continue;
+        const uint32_t qo = rof[q] + x;
+        if (ch.slot == kDirect) Yrow[qo] = acc[i][q][cc];
+        else Prow[qo] = (double)acc[i][q][cc];
+      }
+    }
+  }
+}
+
+// Independent warps: one warp per work item, all of the row's tiles in its
+// lanes' registers; no barrier in the owner loop.
+template <int L, int NTL, typename T>
+__global__ void __launch_bounds__(kThreads, (min_blocks<T, NTL>())) s3ttmc_warp_kernel(const WarpParams p) {
   constexpr bool kExact = sizeof(T) == 8;
+  constexpr int kP = stage_per_lane<L>();
   extern __shared__ __align__(16) unsigned char smem[];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const uint32_t R = p.R, R4 = p.R4;
+  const uint32_t R = p.R, R4 = p.R4, LR4 = (uint32_t)L * R4;
 
-  size_t off = 0;
-  uint32_t *sStart = reinterpret_cast<uint32_t *>(smem + off);
-  off += (((size_t)(L + 1) * (R + 1) * 4) + 15) / 16 * 16;
-  uint8_t *sJ = smem + off;
-  off += ((size_t)p.jtab_len + 15) / 16 * 16;
-  WDesc *sDesc = reinterpret_cast<WDesc *>(smem + off);
-  off += ((size_t)p.ndesc * sizeof(WDesc) + 15) / 16 * 16;
-  T *sWarp = reinterpret_cast<T *>(smem + off);  // kWarps x wsz, later the reduction area
+  const SmemTables tb = load_tables<L>(p, smem, tid, kThreads);
+  if constexpr (L >= 4) __syncthreads();
+  T *sWarp = reinterpret_cast<T *>(tb.rest);  // kWarps x wsz
 
-  if constexpr (L >= 4) {
-    for (uint32_t i = tid; i < (uint32_t)(L + 1) * (R + 1); i += kThreads) sStart[i] = p.starts[i];
-    for (uint32_t i = tid; i < p.jtab_len; i += kThreads) sJ[i] = p.jtab[i];
-    const uint32_t *src = reinterpret_cast<const uint32_t *>(p.desc);
-    uint32_t *dst = reinterpret_cast<uint32_t *>(sDesc);
-    const uint32_t words = p.ndesc * (uint32_t)(sizeof(WDesc) / 4);
-    for (uint32_t i = tid; i < words; i += kThreads) dst[i] = src[i];
-    __syncthreads();
-  }
-
-  // work item: heavy items take the whole CTA, light ones one warp each
-  const bool heavy = blockIdx.x < p.nheavy;
-  const uint32_t item = heavy ? blockIdx.x : p.nheavy + (blockIdx.x - p.nheavy) * kWarps + warp;
-  if (!heavy && item >= p.nchunks) return;  // light CTAs have no barrier below
+  const uint32_t item = blockIdx.x * (uint32_t)kWarps + (uint32_t)warp;
+  if (item >= p.nchunks) return;
   const Chunk ch = p.chunks[item];
 
   // this lane's tiles: 4 consecutive rows r0..r0+3 of block j (all with last
   // index j) times columns x0..x0+3
   int4 tl[NTL];
   bool live[NTL];
+  uint32_t ids[NTL];
 #pragma unroll
   for (int i = 0; i < NTL; ++i) {
-    const uint32_t id = (uint32_t)lane + 32u * i;
-    live[i] = id < p.ntiles;
-    tl[i] = live[i] ? p.tiles[id] : make_int4(0, 0, 0, 0);
+    ids[i] = (uint32_t)lane + 32u * i;
+    live[i] = ids[i] < p.ntiles;
+    tl[i] = live[i] ? p.tiles[ids[i]] : make_int4(0, 0, 0, 0);
   }
 
-  T acc[NTL][4][4], cmp[NTL][4][4], tmp[NTL][4][4];
+  // FP64: the row's sums.  FP32: plain sums of the last kFold owners,
+  // folded into lane-private Kahan pairs in shared memory, so that one
+  // register per output is live across the owner loop.
+  T acc[NTL][4][4];
 #pragma unroll
   for (int i = 0; i < NTL; ++i)
 #pragma unroll
     for (int a = 0; a < 4; ++a)
 #pragma unroll
-      for (int c = 0; c < 4; ++c) { acc[i][a][c] = T(0); cmp[i][a][c] = T(0); tmp[i][a][c] = T(0); }
+      for (int c = 0; c < 4; ++c) acc[i][a][c] = T(0);
+  float2 *sK2 = reinterpret_cast<float2 *>(sWarp + (size_t)kWarps * p.wsz) + (size_t)warp * NTL * 16 * 32;
+  if constexpr (!kExact) {
+#pragma unroll
+    for (int e = 0; e < NTL * 16; ++e) sK2[e * 32 + lane] = make_float2(0.f, 0.f);
+  }
 
   const T *U = reinterpret_cast<const T *>(p.U);
   const T *own_c = reinterpret_cast<const T *>(p.own_c);
@@ -136,179 +318,175 @@ __global__ void __launch_bounds__(kThreads, min_blocks<T>()) s3ttmc_warp_kernel(
   T *sW = sU + L * R4;
   T *sK = sW + L * R4;
   int pending = 0;
-  const uint32_t ostep = heavy ? kWarps : 1;
 
-  for (uint64_t o = ch.ob + (heavy ? warp : 0); o < ch.oe; o += ostep) {
-    // stage the leaf's U rows
-    const uint32_t *S = p.own_S + o * p.sstride;
-    const T c = own_c[o];
-    for (uint32_t i = lane; i < (uint32_t)L * R4; i += 32) {
-      const uint32_t k = i / R4, x = i - k * R4;
-      T u = T(0);
-      if (x < R) u = U[(uint64_t)S[k] * R + x];
-      sU[i] = u;
-      sW[i] = c * u;
+  // Software pipeline over owners: while owner o is computed, the U rows
+  // and coefficient of owner o+1 and the ids of owner o+2 are in flight.
+  // Lane k < L holds id k of an owner; the staging lanes fetch it by shuffle.
+  auto load_ids = [&](uint64_t o) -> uint32_t {
+    return (o < ch.oe && lane < L) ? p.own_S[o * p.sstride + (uint32_t)lane] : 0u;
+  };
+  auto load_rows = [&](uint32_t idv, T (&u)[kP]) {
+#pragma unroll
+    for (int e = 0; e < kP; ++e) {
+      const uint32_t i = (uint32_t)lane + 32u * e, k = i / R4, x = i - k * R4;
+      const uint32_t s = __shfl_sync(0xffffffffu, idv, (int)(k < (uint32_t)L ? k : 0u));
+      u[e] = (i < LR4 && x < R) ? U[(uint64_t)s * R + x] : T(0);
+    }
+  };
+  T u_cur[kP], c_cur = T(0);
+  uint32_t ids_next = 0;
+  if (ch.ob < ch.oe) {
+    load_rows(load_ids(ch.ob), u_cur);
+    c_cur = own_c[ch.ob];
+    ids_next = load_ids(ch.ob + 1);
+  }
+
+  for (uint64_t o = ch.ob; o < ch.oe; ++o) {
+#pragma unroll
+    for (int e = 0; e < kP; ++e) {
+      const uint32_t i = (uint32_t)lane + 32u * e;
+      if (i < LR4) {
+        sU[i] = u_cur[e];
+        sW[i] = c_cur * u_cur[e];
+      }
     }
     __syncwarp();
-    // levels 2 .. L-2 in warp shared memory
+    T u_next[kP], c_next = T(0);
+    const bool more = o + 1 < ch.oe;  // warp-uniform
+    if (more) {
+      load_rows(ids_next, u_next);
+      c_next = own_c[o + 1];
+    } else {
+#pragma unroll
+      for (int e = 0; e < kP; ++e) u_next[e] = T(0);
+    }
+    ids_next = load_ids(o + 2);
     if constexpr (L >= 4) {
 #pragma unroll 1
       for (int d = 2; d <= L - 2; ++d) {
-        const uint32_t md = p.m[d], md4 = p.m4[d], nd = p.desc_count[d];
-        const uint8_t *jt = sJ + p.jtab_off[d];
-        const uint32_t *stt = sStart + d * (R + 1);
-        const WDesc *dd = sDesc + p.desc_begin[d];
-        for (uint32_t it = lane; it < nd * md4; it += 32) {
-          const uint32_t mi = it / md4, e = it - mi * md4;
-          T v = T(0);
-          if (e < md) {
-            const uint32_t j = jt[e], r = e - stt[j];
-            const WDesc &ds = dd[mi];
-#pragma unroll
-            for (int t = 0; t < kMaxL; ++t) {
-              if (t >= d) break;
-              const uint32_t s = ds.src[t];
-              const T a = (s & kURow) ? sU[(s & 0xffu) * R4 + r] : sK[s + r];
-              v += a * sU[ds.k[t] * R4 + j];
-            }
-          }
-          sK[dd[mi].dst + e] = v;
-        }
+        dp_level<L, T>(p, tb, d, sU, sK, (uint32_t)lane, 32u);
         __syncwarp();
       }
     }
-    // last level: the parents K(S \ s_k) at rows (r0+q, j) are
-    //   sum_{t != k} K(S \ {s_k, s_t})[r0+q] * U[s_t][j]
-    // (level N-3 tensors, or U rows for order 4), then the tile gets
-    // sum_k A_k[q] * (c U[s_k])[x0 + cc]
-#pragma unroll
-    for (int i = 0; i < NTL; ++i) {
-      if (!live[i]) continue;
-      const uint32_t r0 = (uint32_t)tl[i].x, jt = (uint32_t)tl[i].y, x0 = (uint32_t)tl[i].z;
-      T w[L][4], uj[L], A[L][4];
-#pragma unroll
-      for (int k = 0; k < L; ++k) ld4(sW + k * R4 + x0, w[k]);
-#pragma unroll
-      for (int t = 0; t < L; ++t) uj[t] = sU[t * R4 + jt];
-      if constexpr (L == 2) {
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          A[0][q] = q == 0 ? uj[1] : T(0);
-          A[1][q] = q == 0 ? uj[0] : T(0);
-        }
-      } else {
-#pragma unroll
-        for (int k = 0; k < L; ++k)
-#pragma unroll
-          for (int q = 0; q < 4; ++q) A[k][q] = T(0);
-#pragma unroll
-        for (int k = 0; k < L; ++k)
-#pragma unroll
-          for (int t = k + 1; t < L; ++t) {
-            const uint32_t s = p.pair_src[pidx(k, t, L)];
-            T kv[4];
-            if constexpr (L == 3) ld4(sU + (s & 0xffu) * R4 + r0, kv);
-            else ld4(sK + s + r0, kv);
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-              A[k][q] += kv[q] * uj[t];
-              A[t][q] += kv[q] * uj[k];
-            }
-          }
-      }
-#pragma unroll
-      for (int q = 0; q < 4; ++q)
-#pragma unroll
-        for (int cc = 0; cc < 4; ++cc) {
-          T s = T(0);
-#pragma unroll
-          for (int k = 0; k < L; ++k) s += A[k][q] * w[k][cc];
-          if constexpr (kExact) acc[i][q][cc] += s;
-          else tmp[i][q][cc] += s;
-        }
-    }
+    tile_step<L, NTL, T>(p, sU, sW, sK, tl, live, acc);
     if constexpr (!kExact) {
-      if (++pending == 4) {
+      if (++pending == kFold) {
         pending = 0;
-#pragma unroll
-        for (int i = 0; i < NTL; ++i)
-#pragma unroll
-          for (int q = 0; q < 4; ++q)
-#pragma unroll
-            for (int cc = 0; cc < 4; ++cc) {
-              T y = tmp[i][q][cc] - cmp[i][q][cc];
-              T s2 = acc[i][q][cc] + y;
-              cmp[i][q][cc] = (s2 - acc[i][q][cc]) - y;
-              acc[i][q][cc] = s2;
-              tmp[i][q][cc] = T(0);
-            }
+        kahan_fold<NTL, T>(sK2, 32u, (uint32_t)lane, acc);
       }
     }
     __syncwarp();
+#pragma unroll
+    for (int e = 0; e < kP; ++e) u_cur[e] = u_next[e];
+    c_cur = c_next;
   }
   if constexpr (!kExact) {
-#pragma unroll
-    for (int i = 0; i < NTL; ++i)
-#pragma unroll
-      for (int q = 0; q < 4; ++q)
-#pragma unroll
-        for (int cc = 0; cc < 4; ++cc) {
-          T y = tmp[i][q][cc] - cmp[i][q][cc];
-          T s2 = acc[i][q][cc] + y;
-          cmp[i][q][cc] = (s2 - acc[i][q][cc]) - y;
-          acc[i][q][cc] = s2 - cmp[i][q][cc];
-        }
+    kahan_fold<NTL, T>(sK2, 32u, (uint32_t)lane, acc);
+    kahan_result<NTL, T>(sK2, 32u, (uint32_t)lane, acc);
   }
+  write_tiles<NTL, T>(p, ch, tl, live, ids, acc);
+}
 
-  T *Yrow = reinterpret_cast<T *>(p.Y) + (uint64_t)ch.row * p.ldy;
-  double *Prow = p.partials + (uint64_t)ch.slot * p.mL;
-  if (!heavy) {  // one warp owns the whole work item: write from registers
+// Team of the CTA's 4 warps per work item, for rows with more tiles than
+// one warp holds: each thread keeps NTL tiles, and the staging and levels
+// 2..L-2 of each owner are computed once for the CTA.  Owner s moves
+// through an (L-1)-deep pipeline with one barrier per step: staged at
+// step s, level d built at step s+d-1, its tiles added at step s+L-2, each
+// owner in its own buffer (L-1 buffers).
+template <int L, int NTL, typename T>
+__global__ void __launch_bounds__(kThreads, (min_blocks<T, NTL>())) s3ttmc_team_kernel(const WarpParams p) {
+  constexpr bool kExact = sizeof(T) == 8;
+  constexpr int kD = L - 1;  // pipeline depth = buffers
+  extern __shared__ __align__(16) unsigned char smem[];
+  const uint32_t tid = threadIdx.x;
+  const uint32_t R = p.R, R4 = p.R4, LR4 = (uint32_t)L * R4;
+
+  const SmemTables tb = load_tables<L>(p, smem, (int)tid, kThreads);
+  T *sBuf = reinterpret_cast<T *>(tb.rest);  // kD x wsz
+  float2 *sK2 = reinterpret_cast<float2 *>(sBuf + (size_t)kD * p.wsz);
+  const Chunk ch = p.chunks[blockIdx.x];
+
+  int4 tl[NTL];
+  bool live[NTL];
+  uint32_t ids[NTL];
 #pragma unroll
-    for (int i = 0; i < NTL; ++i) {
-      if (!live[i]) continue;
-      const uint4 ro = p.rowoff[(uint32_t)lane + 32u * i];
-      const uint32_t rof[4] = {ro.x, ro.y, ro.z, ro.w};
+  for (int i = 0; i < NTL; ++i) {
+    ids[i] = tid + (uint32_t)kThreads * i;
+    live[i] = ids[i] < p.ntiles;
+    tl[i] = live[i] ? p.tiles[ids[i]] : make_int4(0, 0, 0, 0);
+  }
+  T acc[NTL][4][4];
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        if (rof[q] == kPadRow) continue;
+  for (int i = 0; i < NTL; ++i)
 #pragma unroll
-        for (int cc = 0; cc < 4; ++cc) {
-          const uint32_t x = (uint32_t)tl[i].z + cc;
-          if (x >= R || x < (uint32_t)tl[i].y) continue;
-          const uint32_t qo = rof[q] + x;
-          if (ch.slot == kDirect) Yrow[qo] = acc[i][q][cc];
-          else Prow[qo] = (double)acc[i][q][cc];
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int c = 0; c < 4; ++c) acc[i][a][c] = T(0);
+  if constexpr (!kExact) {
+#pragma unroll
+    for (int e = 0; e < NTL * 16; ++e) sK2[e * kThreads + tid] = make_float2(0.f, 0.f);
+  }
+  __syncthreads();
+
+  const T *U = reinterpret_cast<const T *>(p.U);
+  const T *own_c = reinterpret_cast<const T *>(p.own_c);
+  const uint64_t nown = ch.oe - ch.ob;
+  // staging thread tid < L*R4 owns element (k, x) of every owner; the U
+  // value and coefficient of the next owner and the id of the one after
+  // are loaded one step ahead
+  const bool stager = tid < LR4;
+  const uint32_t sk = stager ? tid / R4 : 0u, sx = stager ? tid - sk * R4 : 0u;
+  auto load_id = [&](uint64_t o) -> uint32_t {
+    return (stager && o < nown) ? p.own_S[(ch.ob + o) * p.sstride + sk] : 0u;
+  };
+  T u_n = T(0), c_n = T(0);
+  if (nown) {
+    const uint32_t id0 = load_id(0);
+    if (stager && sx < R) u_n = U[(uint64_t)id0 * R + sx];
+    c_n = own_c[ch.ob];
+  }
+  uint32_t id_n = load_id(1);
+  int pending = 0;
+
+  for (uint64_t s = 0; s < nown + kD - 1; ++s) {
+    if (s < nown) {  // stage owner s into buffer s % kD
+      T *b = sBuf + (size_t)(s % kD) * p.wsz;
+      if (stager) {
+        b[tid] = u_n;
+        b[LR4 + tid] = c_n * u_n;
+      }
+      if (s + 1 < nown) {
+        u_n = (stager && sx < R) ? U[(uint64_t)id_n * R + sx] : T(0);
+        c_n = own_c[ch.ob + s + 1];
+      }
+      id_n = load_id(s + 2);
+    }
+    if constexpr (L >= 4) {
+#pragma unroll 1
+      for (int d = 2; d <= L - 2; ++d) {  // level d of owner s - (d - 1)
+        if (s >= (uint64_t)(d - 1) && s - (d - 1) < nown) {
+          T *b = sBuf + (size_t)((s - (d - 1)) % kD) * p.wsz;
+          dp_level<L, T>(p, tb, d, b, b + 2 * LR4, tid, kThreads);
         }
       }
     }
-    return;
+    if (s >= (uint64_t)(kD - 1)) {  // tiles of owner s - (kD - 1)
+      const T *b = sBuf + (size_t)((s - (kD - 1)) % kD) * p.wsz;
+      tile_step<L, NTL, T>(p, b, b + LR4, b + 2 * LR4, tl, live, acc);
+      if constexpr (!kExact) {
+        if (++pending == kFold) {
+          pending = 0;
+          kahan_fold<NTL, T>(sK2, (uint32_t)kThreads, tid, acc);
+        }
+      }
+    }
+    __syncthreads();
   }
-  // heavy: add the warps' tiles in warp order
-  __syncthreads();
-  T *red = sWarp;  // kWarps x ntiles x 16
-#pragma unroll
-  for (int i = 0; i < NTL; ++i) {
-    if (!live[i]) continue;
-    T *dst = red + ((size_t)warp * p.ntiles + (uint32_t)lane + 32u * i) * 16;
-#pragma unroll
-    for (int q = 0; q < 4; ++q)
-#pragma unroll
-      for (int cc = 0; cc < 4; ++cc) dst[q * 4 + cc] = acc[i][q][cc];
+  if constexpr (!kExact) {
+    kahan_fold<NTL, T>(sK2, (uint32_t)kThreads, tid, acc);
+    kahan_result<NTL, T>(sK2, (uint32_t)kThreads, tid, acc);
   }
-  __syncthreads();
-  for (uint32_t e = tid; e < p.ntiles * 16; e += kThreads) {
-    const uint32_t tile = e >> 4, q = (e >> 2) & 3, cc = e & 3;
-    const int4 tt = p.tiles[tile];
-    const uint32_t x = (uint32_t)tt.z + cc;
-    const uint4 ro = p.rowoff[tile];
-    const uint32_t rof = q == 0 ? ro.x : q == 1 ? ro.y : q == 2 ? ro.z : ro.w;
-    if (rof == kPadRow || x >= R || x < (uint32_t)tt.y) continue;
-    T s = T(0);
-#pragma unroll
-    for (int w2 = 0; w2 < kWarps; ++w2) s += red[((size_t)w2 * p.ntiles + tile) * 16 + (e & 15)];
-    if (ch.slot == kDirect) Yrow[rof + x] = s;
-    else Prow[rof + x] = (double)s;
-  }
+  write_tiles<NTL, T>(p, ch, tl, live, ids, acc);
 }
 
 }  // namespace
@@ -316,6 +494,7 @@ __global__ void __launch_bounds__(kThreads, min_blocks<T>()) s3ttmc_warp_kernel(
 struct WarpPlan {
   bool ok = false;
   uint32_t L = 0, R = 0, R4 = 0, NTL = 0;
+  bool team = false;  // team kernel (4 warps per work item) instead of one warp
   uint32_t m[kMaxL + 1] = {}, m4[kMaxL + 1] = {};
   DBuf<uint32_t> starts;
   DBuf<uint8_t> jtab;
@@ -377,8 +556,17 @@ std::shared_ptr<WarpPlan> warp_plan(uint32_t N, uint32_t R) {
     }
   }
   pl->ntiles = (uint32_t)tiles.size();
-  pl->NTL = (pl->ntiles + 31) / 32;
+  // one warp per work item while the tiles fit 3 per lane (independent
+  // warps, no barrier); beyond that the CTA's 4 warps form a team with up to
+  // 4 tiles per thread
+  pl->team = pl->ntiles > 96;
+  const uint32_t slots = pl->team ? (uint32_t)kThreads : 32u;
+  pl->NTL = (pl->ntiles + slots - 1) / slots;
   if (pl->NTL > (uint32_t)kMaxNTL) return pl;
+  // staging: the warp kernel stages stage_per_lane<L>() values per lane,
+  // the team kernel one per thread
+  if (!pl->team && L * pl->R4 > (L <= 2 ? 128u : 64u)) return pl;
+  if (pl->team && L * pl->R4 > (uint32_t)kThreads) return pl;
   // jtab and descriptors for levels 2..L-2
   std::vector<uint8_t> jt;
   for (uint32_t d = 2; d + 2 <= L; ++d) {
@@ -425,7 +613,10 @@ std::shared_ptr<WarpPlan> warp_plan(uint32_t N, uint32_t R) {
     const size_t es = pi == 0 ? 8 : 4;
     size_t fixed = (((size_t)(L + 1) * (R + 1) * 4) + 15) / 16 * 16 + ((size_t)pl->jtab_len + 15) / 16 * 16 +
                    ((size_t)pl->ndesc * sizeof(WDesc) + 15) / 16 * 16;
-    size_t work = std::max((size_t)kWarps * pl->wsz * es, (size_t)kWarps * pl->ntiles * 16 * es);
+    // warp kernel: one staging area per warp; team kernel: one per
+    // pipeline stage (L-1); FP32 adds the Kahan pairs of every thread
+    size_t work = (size_t)(pl->team ? L - 1 : kWarps) * pl->wsz * es;
+    if (pi == 1) work = (work + 15) / 16 * 16 + (size_t)kThreads * pl->NTL * 16 * sizeof(float) * 2;
     pl->smem[pi] = fixed + work;
     if (pl->smem[pi] > 200 * 1024) return pl;
   }
@@ -445,35 +636,38 @@ std::shared_ptr<WarpPlan> warp_plan(uint32_t N, uint32_t R) {
 }
 
 bool warp_supported(const WarpPlan &pl) { return pl.ok; }
+bool warp_preferred(const WarpPlan &pl) { return pl.ok; }
 
 template <int L, int NTL, typename T>
-static void launch_w(const WarpParams &wp, uint32_t grid, size_t smem, cudaStream_t st) {
-  auto kern = s3ttmc_warp_kernel<L, NTL, T>;
+static void launch_w(bool team, const WarpParams &wp, uint32_t nchunks, size_t smem, cudaStream_t st) {
+  auto kern = team ? s3ttmc_team_kernel<L, NTL, T> : s3ttmc_warp_kernel<L, NTL, T>;
+  const uint32_t grid = team ? nchunks : (nchunks + kWarps - 1) / kWarps;
   SPB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   kern<<<grid, kThreads, smem, st>>>(wp);
   SPB_LAUNCH_CHECK();
 }
 
 template <int L, typename T>
-static void launch_w_ntl(uint32_t NTL, const WarpParams &wp, uint32_t grid, size_t smem, cudaStream_t st) {
+static void launch_w_ntl(uint32_t NTL, bool team, const WarpParams &wp, uint32_t nchunks, size_t smem,
+                         cudaStream_t st) {
   switch (NTL) {
-    case 1: launch_w<L, 1, T>(wp, grid, smem, st); break;
-    case 2: launch_w<L, 2, T>(wp, grid, smem, st); break;
-    case 3: launch_w<L, 3, T>(wp, grid, smem, st); break;
-    default: launch_w<L, 4, T>(wp, grid, smem, st); break;
+    case 1: launch_w<L, 1, T>(team, wp, nchunks, smem, st); break;
+    case 2: launch_w<L, 2, T>(team, wp, nchunks, smem, st); break;
+    case 3: launch_w<L, 3, T>(team, wp, nchunks, smem, st); break;
+    default: launch_w<L, 4, T>(team, wp, nchunks, smem, st); break;
   }
 }
 
 template <typename T>
-static void launch_w_l(uint32_t L, uint32_t NTL, const WarpParams &wp, uint32_t grid, size_t smem,
+static void launch_w_l(uint32_t L, uint32_t NTL, bool team, const WarpParams &wp, uint32_t nchunks, size_t smem,
                        cudaStream_t st) {
   switch (L) {
-    case 2: launch_w_ntl<2, T>(NTL, wp, grid, smem, st); break;
-    case 3: launch_w_ntl<3, T>(NTL, wp, grid, smem, st); break;
-    case 4: launch_w_ntl<4, T>(NTL, wp, grid, smem, st); break;
-    case 5: launch_w_ntl<5, T>(NTL, wp, grid, smem, st); break;
-    case 6: launch_w_ntl<6, T>(NTL, wp, grid, smem, st); break;
-    default: launch_w_ntl<7, T>(NTL, wp, grid, smem, st); break;
+    case 2: launch_w_ntl<2, T>(NTL, team, wp, nchunks, smem, st); break;
+    case 3: launch_w_ntl<3, T>(NTL, team, wp, nchunks, smem, st); break;
+    case 4: launch_w_ntl<4, T>(NTL, team, wp, nchunks, smem, st); break;
+    case 5: launch_w_ntl<5, T>(NTL, team, wp, nchunks, smem, st); break;
+    case 6: launch_w_ntl<6, T>(NTL, team, wp, nchunks, smem, st); break;
+    default: launch_w_ntl<7, T>(NTL, team, wp, nchunks, smem, st); break;
   }
 }
 
@@ -484,7 +678,6 @@ void warp_launch(const WarpPlan &pl, const TensorState &t, const void *dU, void 
   WarpParams wp{};
   wp.chunks = t.chunks.p;
   wp.nchunks = t.nchunks;
-  wp.nheavy = t.nheavy;
   wp.own_S = t.own_S.p;
   wp.own_c = pi == 0 ? (const void *)t.own_c64.p : (const void *)t.own_c32.p;
   wp.sstride = t.sstride;
@@ -512,10 +705,8 @@ void warp_launch(const WarpPlan &pl, const TensorState &t, const void *dU, void 
   wp.rowoff = pl.rowoff.p;
   wp.ntiles = pl.ntiles;
   wp.wsz = pl.wsz;
-  const uint32_t nlight = t.nchunks - t.nheavy;
-  const uint32_t grid = t.nheavy + (nlight + kWarps - 1) / kWarps;
-  if (pi == 0) launch_w_l<double>(pl.L, pl.NTL, wp, grid, pl.smem[0], st);
-  else launch_w_l<float>(pl.L, pl.NTL, wp, grid, pl.smem[1], st);
+  if (pi == 0) launch_w_l<double>(pl.L, pl.NTL, pl.team, wp, t.nchunks, pl.smem[0], st);
+  else launch_w_l<float>(pl.L, pl.NTL, pl.team, wp, t.nchunks, pl.smem[1], st);
 }
 
 }  // namespace spb
