@@ -324,7 +324,7 @@ __global__ void __launch_bounds__(1024) jacobi_kernel(const double *S, int n, do
   __shared__ int pr[2 * 64];
   __shared__ int order[128];
   __shared__ double red[1024];
-  const int tid = threadIdx.x, nt = blockDim.x;
+  const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5, nwarp = nt >> 5;
   for (int idx = tid; idx < np * np; idx += nt) {
     int i = idx / np, j = idx % np;
     A[i * ld + j] = (i < n && j < n) ? S[i * n + j] : 0.0;
@@ -367,25 +367,29 @@ __global__ void __launch_bounds__(1024) jacobi_kernel(const double *S, int n, do
         cs[2 * k + 1] = s;
       }
       __syncthreads();
-      for (int idx = tid; idx < half * np; idx += nt) {  // rows: A <- J^T A
-        int k = idx / np, col = idx % np;
-        int p = pr[2 * k], q = pr[2 * k + 1];
-        double c = cs[2 * k], s = cs[2 * k + 1];
-        double a = A[p * ld + col], b = A[q * ld + col];
-        A[p * ld + col] = c * a - s * b;
-        A[q * ld + col] = s * a + c * b;
+      // warp w applies rotations w, w+32, ...; its lanes stride the rows or
+      // columns (no integer division in the sweep)
+      for (int k = warp; k < half; k += nwarp) {  // rows: A <- J^T A
+        const int p = pr[2 * k], q = pr[2 * k + 1];
+        const double c = cs[2 * k], s = cs[2 * k + 1];
+        for (int col = lane; col < np; col += 32) {
+          const double a = A[p * ld + col], b = A[q * ld + col];
+          A[p * ld + col] = c * a - s * b;
+          A[q * ld + col] = s * a + c * b;
+        }
       }
       __syncthreads();
-      for (int idx = tid; idx < half * np; idx += nt) {  // cols: A <- A J, V <- V J
-        int k = idx / np, row = idx % np;
-        int p = pr[2 * k], q = pr[2 * k + 1];
-        double c = cs[2 * k], s = cs[2 * k + 1];
-        double a = A[row * ld + p], b = A[row * ld + q];
-        A[row * ld + p] = c * a - s * b;
-        A[row * ld + q] = s * a + c * b;
-        double va = V[row * ld + p], vb = V[row * ld + q];
-        V[row * ld + p] = c * va - s * vb;
-        V[row * ld + q] = s * va + c * vb;
+      for (int k = warp; k < half; k += nwarp) {  // cols: A <- A J, V <- V J
+        const int p = pr[2 * k], q = pr[2 * k + 1];
+        const double c = cs[2 * k], s = cs[2 * k + 1];
+        for (int row = lane; row < np; row += 32) {
+          const double a = A[row * ld + p], b = A[row * ld + q];
+          A[row * ld + p] = c * a - s * b;
+          A[row * ld + q] = s * a + c * b;
+          const double va = V[row * ld + p], vb = V[row * ld + q];
+          V[row * ld + p] = c * va - s * vb;
+          V[row * ld + q] = s * va + c * vb;
+        }
       }
       __syncthreads();
     }
@@ -651,7 +655,10 @@ int top_eigs(cudaStream_t st, const double *S, int s, int r, double *V, double *
   }
   const int b = std::min(std::max(r + 8, 2 * r), std::min(48, s));
   if (b < r) fail(SYMPROP_ERR_SIZE, "rank %d too large for the eigensolver", r);
-  const int nblk = std::max(2, kJacobiMax / b);
+  // Krylov basis of at most kKrylovCols columns (the Rayleigh-Ritz Jacobi
+  // costs O(nb^3) per restart); at least two blocks
+  constexpr int kKrylovCols = 64;
+  const int nblk = std::max(2, kKrylovCols / b);
   const int nb = nblk * b;  // Krylov basis width
   Scratch Q(sizeof(double) * (size_t)s * nb, st), SQ(sizeof(double) * (size_t)s * nb, st),
       T(sizeof(double) * nb * nb, st), w(sizeof(double) * nb, st), Z(sizeof(double) * nb * nb, st),

@@ -27,6 +27,7 @@
 // permutation table).  FP32 mode folds the lane's plain FP32 sums into a
 // Kahan-compensated accumulator in shared memory every 8 owners.
 #include <algorithm>
+#include <utility>
 
 #include "s3ttmc_warp.cuh"
 
@@ -60,6 +61,7 @@ struct WarpParams {
   uint32_t jtab_len, jtab_off[kMaxL + 1];
   const WDesc *desc;
   uint32_t ndesc, desc_begin[kMaxL + 1], desc_count[kMaxL + 1];
+  uint32_t lvl_off[kMaxL + 1];  // offset of the first level-d tensor in a staging area
   uint32_t m[kMaxL + 1], m4[kMaxL + 1];
   uint32_t pair_src[kMaxL * kMaxL];  // level N-3 tensor of the positions other than {k,t}
   const int4 *tiles;                 // per tile: (first row r0 inside block j, j, first column x0, 0)
@@ -120,33 +122,88 @@ __device__ __forceinline__ SmemTables load_tables(const WarpParams &p, unsigned 
   return tb;
 }
 
-// One level d (2 <= d <= L-2) of the recursion for one owner: every
-// sub-multiset tensor of order d, colex order, from level d-1 (or U rows)
-// times U; elements strided over nthr threads.
-template <int L, typename T>
-__device__ __forceinline__ void dp_level(const WarpParams &p, const SmemTables &tb, int d, const T *sU, T *sK,
-                                         uint32_t tid, uint32_t nthr) {
-  const uint32_t R4 = p.R4;
-  const uint32_t md = p.m[d], md4 = p.m4[d], nd = p.desc_count[d];
-  const uint8_t *jt = tb.jt + p.jtab_off[d];
-  const uint32_t *stt = tb.start + d * (p.R + 1);
-  const WDesc *dd = tb.desc + p.desc_begin[d];
-  for (uint32_t it = tid; it < nd * md4; it += nthr) {
-    const uint32_t mi = it / md4, e = it - mi * md4;
-    T v = T(0);
-    if (e < md) {
-      const uint32_t j = jt[e], r = e - stt[j];
-      const WDesc &ds = dd[mi];
-#pragma unroll
-      for (int t = 0; t < kMaxL; ++t) {
-        if (t >= d) break;
-        const uint32_t s = ds.src[t];
-        const T a = (s & kURow) ? sU[(s & 0xffu) * R4 + r] : sK[s + r];
-        v += a * sU[ds.k[t] * R4 + j];
-      }
+// Compile-time enumeration of the sub-multisets of the leaf's L positions
+// as L-bit masks, in the order the plan lays their tensors out: by
+// popcount, then by increasing mask value.
+__host__ __device__ constexpr int popc(int x) { return x ? (x & 1) + popc(x >> 1) : 0; }
+__host__ __device__ constexpr int mask_at(int L, int d, int i) {  // i-th mask of popcount d
+  int found = 0;
+  for (int m = 0; m < (1 << L); ++m)
+    if (popc(m) == d) {
+      if (found == i) return m;
+      ++found;
     }
-    sK[dd[mi].dst + e] = v;
+  return 0;
+}
+__host__ __device__ constexpr int mask_rank(int L, int m) {  // index among masks of its popcount
+  int r = 0;
+  for (int x = 0; x < m; ++x) r += popc(x) == popc(m) ? 1 : 0;
+  return r + 0 * L;
+}
+__host__ __device__ constexpr int nmasks(int L, int d) {
+  int c = 0;
+  for (int m = 0; m < (1 << L); ++m) c += popc(m) == d ? 1 : 0;
+  return c;
+}
+
+template <int L, int M, int K, int NS, typename T>
+__device__ __forceinline__ void dp_term(T &v, const T (&src)[NS], const T (&uj)[L]) {
+  if constexpr (((M >> K) & 1) != 0) {
+    constexpr int s = mask_rank(L, M & ~(1 << K));
+    v += src[s] * uj[K];
   }
+}
+
+template <int L, int D, int I, int NS, typename T, int... K>
+__device__ __forceinline__ void dp_mask(T *dst, uint32_t stride, uint32_t e, const T (&src)[NS],
+                                        const T (&uj)[L], std::integer_sequence<int, K...>) {
+  constexpr int M = mask_at(L, D, I);
+  T v = T(0);
+  (dp_term<L, M, K, NS, T>(v, src, uj), ...);
+  dst[(uint32_t)I * stride + e] = v;
+}
+
+template <int L, int D, int NS, typename T, int... I>
+__device__ __forceinline__ void dp_masks(T *dst, uint32_t stride, uint32_t e, const T (&src)[NS],
+                                         const T (&uj)[L], std::integer_sequence<int, I...>) {
+  (dp_mask<L, D, I, NS, T>(dst, stride, e, src, uj, std::make_integer_sequence<int, L>{}), ...);
+}
+
+// Level D (2 <= D <= L-2) of the recursion for one owner: every
+// sub-multiset tensor of order D, colex order.  Element e = (row r of
+// block j) of all C(L, D) tensors at once:
+//   K_D(M)[e] = sum_{k in M} K_{D-1}(M \ k)[r] * U[s_k][j],
+// with the C(L, D-1) source values and the L values U[s_k][j] loaded once;
+// elements strided over nthr threads.
+template <int L, int D, typename T>
+__device__ __forceinline__ void dp_level(const WarpParams &p, const SmemTables &tb, const T *sU, T *sK,
+                                         uint32_t tid, uint32_t nthr) {
+  constexpr int NS = nmasks(L, D - 1);
+  const uint32_t R4 = p.R4, md = p.m[D];
+  const uint8_t *jt = tb.jt + p.jtab_off[D];
+  const uint32_t *stt = tb.start + D * (p.R + 1);
+  const T *srcK = sK + p.lvl_off[D - 1];
+  const uint32_t sstr = p.m4[D - 1];
+  T *dst = sK + p.lvl_off[D];
+  for (uint32_t e = tid; e < md; e += nthr) {
+    const uint32_t j = jt[e], r = e - stt[j];
+    T uj[L], src[NS];
+#pragma unroll
+    for (int k = 0; k < L; ++k) uj[k] = sU[k * R4 + j];
+#pragma unroll
+    for (int i = 0; i < NS; ++i) src[i] = (D == 2) ? sU[i * R4 + r] : srcK[i * sstr + r];
+    dp_masks<L, D, NS, T>(dst, p.m4[D], e, src, uj, std::make_integer_sequence<int, nmasks(L, D)>{});
+  }
+}
+
+// dp_level for a level d known at run time (2 <= d <= L-2)
+template <int L, typename T>
+__device__ __forceinline__ void dp_level_rt(int d, const WarpParams &p, const SmemTables &tb, const T *sU, T *sK,
+                                            uint32_t tid, uint32_t nthr) {
+  if constexpr (L >= 4) if (d == 2) dp_level<L, 2, T>(p, tb, sU, sK, tid, nthr);
+  if constexpr (L >= 5) if (d == 3) dp_level<L, 3, T>(p, tb, sU, sK, tid, nthr);
+  if constexpr (L >= 6) if (d == 4) dp_level<L, 4, T>(p, tb, sU, sK, tid, nthr);
+  if constexpr (L >= 7) if (d == 5) dp_level<L, 5, T>(p, tb, sU, sK, tid, nthr);
 }
 
 // The last level for one owner on this thread's tiles: the parents
@@ -318,6 +375,10 @@ __global__ void __launch_bounds__(kThreads, (min_blocks<T, NTL>())) s3ttmc_warp_
   T *sW = sU + L * R4;
   T *sK = sW + L * R4;
   int pending = 0;
+  // the padding rows of the level tensors are read (and discarded) by the
+  // last level: keep them finite
+  for (uint32_t i = lane; i < p.wsz; i += 32) sU[i] = T(0);
+  __syncwarp();
 
   // Software pipeline over owners: while owner o is computed, the U rows
   // and coefficient of owner o+1 and the ids of owner o+2 are in flight.
@@ -364,7 +425,7 @@ __global__ void __launch_bounds__(kThreads, (min_blocks<T, NTL>())) s3ttmc_warp_
     if constexpr (L >= 4) {
 #pragma unroll 1
       for (int d = 2; d <= L - 2; ++d) {
-        dp_level<L, T>(p, tb, d, sU, sK, (uint32_t)lane, 32u);
+        dp_level_rt<L, T>(d, p, tb, sU, sK, (uint32_t)lane, 32u);
         __syncwarp();
       }
     }
@@ -426,6 +487,9 @@ __global__ void __launch_bounds__(kThreads, (min_blocks<T, NTL>())) s3ttmc_team_
 #pragma unroll
     for (int e = 0; e < NTL * 16; ++e) sK2[e * kThreads + tid] = make_float2(0.f, 0.f);
   }
+  // the padding rows of the level tensors are read (and discarded) by the
+  // last level: keep them finite
+  for (uint32_t i = tid; i < (uint32_t)kD * p.wsz; i += kThreads) sBuf[i] = T(0);
   __syncthreads();
 
   const T *U = reinterpret_cast<const T *>(p.U);
@@ -466,7 +530,7 @@ __global__ void __launch_bounds__(kThreads, (min_blocks<T, NTL>())) s3ttmc_team_
       for (int d = 2; d <= L - 2; ++d) {  // level d of owner s - (d - 1)
         if (s >= (uint64_t)(d - 1) && s - (d - 1) < nown) {
           T *b = sBuf + (size_t)((s - (d - 1)) % kD) * p.wsz;
-          dp_level<L, T>(p, tb, d, b, b + 2 * LR4, tid, kThreads);
+          dp_level_rt<L, T>(d, p, tb, b, b + 2 * LR4, tid, kThreads);
         }
       }
     }
@@ -500,7 +564,7 @@ struct WarpPlan {
   DBuf<uint8_t> jtab;
   uint32_t jtab_len = 0, jtab_off[kMaxL + 1] = {};
   DBuf<WDesc> desc;
-  uint32_t ndesc = 0, desc_begin[kMaxL + 1] = {}, desc_count[kMaxL + 1] = {};
+  uint32_t ndesc = 0, desc_begin[kMaxL + 1] = {}, desc_count[kMaxL + 1] = {}, lvl_off[kMaxL + 1] = {};
   uint32_t pair_src[kMaxL * kMaxL] = {};
   DBuf<int4> tiles;
   DBuf<uint4> rowoff;
@@ -581,6 +645,7 @@ std::shared_ptr<WarpPlan> warp_plan(uint32_t N, uint32_t R) {
   uint32_t ksz = 0;
   for (uint32_t d = 2; d + 2 <= L; ++d) {
     pl->desc_begin[d] = (uint32_t)desc.size();
+    pl->lvl_off[d] = ksz;  // masks of popcount d follow in increasing order (dp_level relies on it)
     for (uint32_t mask = 0; mask < (1u << L); ++mask) {
       if ((uint32_t)__builtin_popcount(mask) != d) continue;
       WDesc ds{};
@@ -598,7 +663,9 @@ std::shared_ptr<WarpPlan> warp_plan(uint32_t N, uint32_t R) {
     }
     pl->desc_count[d] = (uint32_t)desc.size() - pl->desc_begin[d];
   }
-  pl->ndesc = (uint32_t)desc.size();
+  // the kernels enumerate the masks at compile time: the descriptors only
+  // fix the offsets above and are not uploaded
+  pl->ndesc = 0;
   pl->ksz4 = ksz;
   if (L >= 3) {
     for (uint32_t k = 0; k < L; ++k)
@@ -697,6 +764,7 @@ void warp_launch(const WarpPlan &pl, const TensorState &t, const void *dU, void 
     wp.jtab_off[d] = pl.jtab_off[d];
     wp.desc_begin[d] = pl.desc_begin[d];
     wp.desc_count[d] = pl.desc_count[d];
+    wp.lvl_off[d] = pl.lvl_off[d];
     wp.m[d] = pl.m[d];
     wp.m4[d] = pl.m4[d];
   }
