@@ -41,6 +41,15 @@ sys.path.insert(0, ROOT)
 
 WORKLOAD = "s3ttmc_order4_zipf"
 RANK = 16
+# --workload choices: the S3TTMc-alone workload (the default bench line) and
+# the S3TTMc of the two HOOI workloads with wide packed rows
+WORKLOADS = {
+    "s3ttmc_order4_zipf": (16, "order 4, n=100000, 5M tuples, Zipf(1.1), values uniform (0,1]"),
+    "learned_order5_powerlaw": (16, "order 5, n=200000, 20M tuples, power-law degrees (exponent 2.1), "
+                                    "16 planted communities, values 1.0"),
+    "mixed_order6_planted": (10, "order 6, n=50000, 2M tuples, 8 planted communities (80% inside), "
+                                 "values 1.0"),
+}
 METRIC = "S3TTMc algorithmic GB/s"
 REF_SAMPLE_NNZ = 250_000   # bounded sample for the CPU reference (~1 s per call on 8 cores)
 
@@ -169,6 +178,10 @@ def run_reference(args):
     if not os.path.exists(probe):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_probe not built"}))
         return 0
+    if WORKLOAD != "s3ttmc_order4_zipf":
+        print(json.dumps({"impl": "reference", "unavailable": "the reference arm times the order-4 S3TTMc "
+                          "workload only (the reference materialises the level N-2 array: OOM at order 5/6)"}))
+        return 0
     order, n, t, v = synth.workload(WORKLOAD, scale=REF_SAMPLE_NNZ / 5_000_000)
     nnz = t.shape[0]
     tmp = tempfile.mkdtemp()
@@ -188,12 +201,12 @@ def run_reference(args):
     line = {"impl": "reference", "metric": METRIC, "value": round(val, 4), "unit": "GB/s",
             "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_step, 3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic (seeded Zipf(1.1) generator)",
-            "config": {"workload": f"{WORKLOAD}: order 4, n=100000, Zipf(1.1), R=16, packed Y",
+            "data": "synthetic (seeded generator)",
+            "config": {"workload": f"{WORKLOAD}: {WORKLOADS[WORKLOAD][1]}, R={RANK}, packed Y",
                        "sample_nnz": nnz, "levels": levels},
             "cpu_baseline": {"value": round(val, 4), "unit": "GB/s", "cores": int(js["threads"]),
                              "kind": "reference",
-                             "sample": f"{nnz} tuples of the workload's distribution (n=100000), "
+                             "sample": f"{nnz} tuples of the workload's distribution (n={n}), "
                                        f"S3TTMc(packed) per step; build {js['build_ms']:.0f} ms excluded"},
             "e2e": {"value": round(val, 4), "unit": "GB/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
@@ -213,6 +226,7 @@ def tree_levels_cpu(order, n, t, v):
 
 
 def main():
+    global WORKLOAD, RANK
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
@@ -221,11 +235,14 @@ def main():
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default=WORKLOAD, choices=sorted(WORKLOADS))
     ap.add_argument("--scale", type=float, default=1.0,
                     help="fraction of the workload's tuples (small cases for profiling only)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    WORKLOAD = args.workload
+    RANK = WORKLOADS[WORKLOAD][0]
     if args.impl == "reference":
         return run_reference(args)
 
@@ -324,7 +341,7 @@ def main():
     traffic = load_traffic(args.precision)
     clocks = clk.summary()
     cpu = None
-    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline and WORKLOAD == "s3ttmc_order4_zipf":
         cpu = cpu_baseline()
     if rank == 0:
         line = {
@@ -332,8 +349,8 @@ def main():
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_step, 4),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64" if prec == sp.FP64 else "f32",
-            "data": "synthetic (seeded Zipf(1.1) generator, values uniform (0,1])",
-            "config": {"workload": f"{WORKLOAD}: order 4, n=100000, nnz={nnz}, Zipf(1.1), R=16, "
+            "data": "synthetic (seeded generator of the workload; no dataset is shipped)",
+            "config": {"workload": f"{WORKLOAD}: {WORKLOADS[WORKLOAD][1]}, nnz={nnz}, R={RANK}, "
                                    f"Y packed n x {m}", "parallelism": f"replicas x{ws}",
                        "levels": levels, "owners_after_merge": X.owner_count(),
                        "alg_bytes_per_step": B, "alg_flops_per_step": F,

@@ -53,7 +53,11 @@ def main():
     ap.add_argument("--delta", type=float, default=1.0)
     ap.add_argument("--weights", default=None)
     ap.add_argument("--reference", action="store_true")
+    ap.add_argument("--arms", default="fp64_random,mixed_random,mixed_learned,fp64_learned",
+                    help="comma list of fp64_random, mixed_random, mixed_learned, fp64_learned")
+    ap.add_argument("--no-warmup", action="store_true", help="skip the untimed first solve")
     a = ap.parse_args()
+    arms = set(a.arms.split(","))
     order, n, t, v = synth.workload(a.workload, scale=a.scale)
     X = SpSymtensor(n, order, t, v)
     rows = []
@@ -69,32 +73,37 @@ def main():
         print(json.dumps(row))
         return d
 
-    solve("warmup", PREC_FP64)  # first-use plans and module loading
-    rows.clear()
-    ref64 = solve("fp64_random", PREC_FP64)
-    solve("mixed_random", PREC_MIXED)
+    if not a.no_warmup:
+        solve("warmup", PREC_FP64)  # first-use plans and module loading
+        rows.clear()
+    ref64 = solve("fp64_random", PREC_FP64) if "fp64_random" in arms else None
+    if "mixed_random" in arms:
+        solve("mixed_random", PREC_MIXED)
     wpath = a.weights
     if wpath is None:
         cand = os.path.join(os.path.dirname(os.path.abspath(__file__)), f"warmstart_r{a.rank}.npz")
         wpath = cand if os.path.exists(cand) else None
-    if wpath:
+    if wpath and arms & {"mixed_learned", "fp64_learned"}:
         from .warmstart import WarmStartModel
         model = WarmStartModel.load(wpath)
         t0 = time.perf_counter()
         U0 = model.predict(X, seed=0)
         pred_ms = (time.perf_counter() - t0) * 1e3
-        solve("mixed_learned", PREC_MIXED, U0=U0, extra_ms=pred_ms)
-        solve("fp64_learned", PREC_FP64, U0=U0, extra_ms=pred_ms)
+        if "mixed_learned" in arms:
+            solve("mixed_learned", PREC_MIXED, U0=U0, extra_ms=pred_ms)
+        if "fp64_learned" in arms:
+            solve("fp64_learned", PREC_FP64, U0=U0, extra_ms=pred_ms)
     if a.reference:
         r = run_ref(order, n, t, v, a.rank, a.iters, a.tol, a.delta)
         if r:
             rows.append(r)
             print(json.dumps(r))
     summ = {"workload": a.workload, "scale": a.scale, "order": order, "n": n, "nnz": int(t.shape[0]),
-            "rank": a.rank, "tol": a.tol, "delta": a.delta,
-            "speedup_vs_fp64_random": {r["arm"]: round(ref64.time_ms / r["ms"], 3) for r in rows if r["ms"]},
-            "objective_rel_gap_vs_fp64": {r["arm"]: (abs(r["error"] - ref64.error) / ref64.error
-                                                   if r["error"] is not None else None) for r in rows}}
+            "rank": a.rank, "tol": a.tol, "delta": a.delta}
+    if ref64 is not None:
+        summ["speedup_vs_fp64_random"] = {r["arm"]: round(ref64.time_ms / r["ms"], 3) for r in rows if r["ms"]}
+        summ["objective_rel_gap_vs_fp64"] = {r["arm"]: (abs(r["error"] - ref64.error) / ref64.error
+                                                        if r["error"] is not None else None) for r in rows}
     print(json.dumps(summ))
 
 

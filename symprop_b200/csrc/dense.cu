@@ -324,6 +324,7 @@ __global__ void __launch_bounds__(1024) jacobi_kernel(const double *S, int n, do
   __shared__ int pr[2 * 64];
   __shared__ int order[128];
   __shared__ double red[1024];
+  __shared__ int rotated;
   const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5, nwarp = nt >> 5;
   for (int idx = tid; idx < np * np; idx += nt) {
     int i = idx / np, j = idx % np;
@@ -346,6 +347,8 @@ __global__ void __launch_bounds__(1024) jacobi_kernel(const double *S, int n, do
     }
     off = block_sum(off, red);
     if (!(off > 1e-30 * fro)) break;
+    if (tid == 0) rotated = 0;
+    __syncthreads();
     for (int step = 0; step < np - 1; ++step) {
       if (tid < half) {
         int k = tid;
@@ -355,10 +358,15 @@ __global__ void __launch_bounds__(1024) jacobi_kernel(const double *S, int n, do
         int p = min(a, b), q = max(a, b);
         pr[2 * k] = p;
         pr[2 * k + 1] = q;
-        double apq = A[p * ld + q];
+        const double apq = A[p * ld + q], app = A[p * ld + p], aqq = A[q * ld + q];
         double c = 1.0, s = 0.0;
-        if (apq != 0.0) {
-          double tau = (A[q * ld + q] - A[p * ld + p]) / (2.0 * apq);
+        // an element below the rounding level of its diagonal pair (or of
+        // the whole matrix) is left alone; a sweep that rotates nothing ends
+        // the iteration (rounding noise keeps off() from reaching zero)
+        const bool negligible = fabs(apq) <= 1e-17 * sqrt(fabs(app * aqq)) || fabs(apq) <= 1e-18 * sqrt(fro);
+        if (!negligible) {
+          rotated = 1;
+          double tau = (aqq - app) / (2.0 * apq);
           double t = (tau >= 0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
           c = 1.0 / sqrt(1.0 + t * t);
           s = t * c;
@@ -393,6 +401,7 @@ __global__ void __launch_bounds__(1024) jacobi_kernel(const double *S, int n, do
       }
       __syncthreads();
     }
+    if (rotated == 0) break;
   }
   // sort eigenvalues descending (only the first n indices are real)
   if (tid == 0) {
@@ -558,6 +567,9 @@ void householder_q(cudaStream_t st, double *A, int rows, int cols) {
   SPB_CUDA(cudaMemcpyAsync(A, Q.p, sizeof(double) * (size_t)rows * cols, cudaMemcpyDeviceToDevice, st));
 }
 
+// CholQR2 calls that fell back to Householder QR (reported by the trace)
+static int g_householder_fallbacks = 0;
+
 bool orthonormalize(cudaStream_t st, double *A, int rows, int cols) {
   if (cols > 64 || rows < cols) {
     householder_q(st, A, rows, cols);
@@ -583,6 +595,7 @@ bool orthonormalize(cudaStream_t st, double *A, int rows, int cols) {
   SPB_CUDA(cudaMemcpyAsync(hstat, stat.p, sizeof(int) * 2, cudaMemcpyDeviceToHost, st));
   SPB_CUDA(cudaStreamSynchronize(st));
   if (hstat[0] || hstat[1]) {
+    ++g_householder_fallbacks;
     // Gram matrix numerically singular: restart from the original columns
     // with Householder QR, which is stable for any conditioning.
     SPB_CUDA(cudaMemcpyAsync(A, orig.p, sizeof(double) * (size_t)rows * cols, cudaMemcpyDeviceToDevice, st));
@@ -655,10 +668,11 @@ int top_eigs(cudaStream_t st, const double *S, int s, int r, double *V, double *
   }
   const int b = std::min(std::max(r + 8, 2 * r), std::min(48, s));
   if (b < r) fail(SYMPROP_ERR_SIZE, "rank %d too large for the eigensolver", r);
-  // Krylov basis of at most kKrylovCols columns (the Rayleigh-Ritz Jacobi
-  // costs O(nb^3) per restart); at least two blocks
-  constexpr int kKrylovCols = 64;
-  const int nblk = std::max(2, kKrylovCols / b);
+  // Krylov basis width: the Rayleigh-Ritz Jacobi costs O(nb^3) per restart
+  // whatever s is, the products with S O(s^2 nb): small matrices take 64
+  // columns, large ones the full 96 (fewer restarts); at least two blocks
+  const int krylov_cols = s < 1024 ? 64 : kJacobiMax;
+  const int nblk = std::max(2, krylov_cols / b);
   const int nb = nblk * b;  // Krylov basis width
   Scratch Q(sizeof(double) * (size_t)s * nb, st), SQ(sizeof(double) * (size_t)s * nb, st),
       T(sizeof(double) * nb * nb, st), w(sizeof(double) * nb, st), Z(sizeof(double) * nb * nb, st),
@@ -721,8 +735,9 @@ int top_eigs(cudaStream_t st, const double *S, int s, int r, double *V, double *
     for (int i = 0; i < r; ++i) worst = std::max(worst, hres[i] / scale);
     if (worst <= tol || it == max_restarts) {
       if (eig_trace())
-        std::fprintf(stderr, "top_eigs: s=%d r=%d b=%d restarts=%d residual=%.3e tol=%.1e\n", s, r, b, it,
-                     worst, tol);
+        std::fprintf(stderr, "top_eigs: s=%d r=%d b=%d restarts=%d residual=%.3e tol=%.1e householder=%d\n", s, r,
+                     b, it, worst, tol, g_householder_fallbacks);
+      g_householder_fallbacks = 0;
       copy_cols_kernel<<<cdiv((long long)s * r, 256), 256, 0, st>>>(X.as<double>(), b, s, r, V, r);
       SPB_LAUNCH_CHECK();
       for (int i = 0; i < r; ++i) lam[i] = hw[i];

@@ -27,19 +27,22 @@ def main():
     ap.add_argument("--rank", type=int, default=8)
     ap.add_argument("--hidden", type=int, default=64)
     ap.add_argument("--full-size", action="store_true", help="n up to 20k, nnz up to 500k")
+    ap.add_argument("--family", default="community", choices=["community", "powerlaw"],
+                    help="training tensors: planted-community Zipf (orders 3-6) or order-5 power-law")
     ap.add_argument("--out", default=ws.DEFAULT_WEIGHTS)
     ap.add_argument("--report", default=None)
     a = ap.parse_args()
     t0 = time.time()
-    samples = ws.make_samples(range(a.count), R=a.rank, small=not a.full_size)
+    samples = ws.make_samples(range(a.count), R=a.rank, small=not a.full_size, family=a.family)
     t1 = time.time()
     model = ws.WarmStartModel(a.rank, a.hidden, seed=0)
     hist = ws.train(model, samples, epochs=a.epochs, lr=a.lr)
     t2 = time.time()
     model.save(a.out)
-    rows = ws.compare(model, range(5000, 5000 + a.heldout), R=a.rank, small=not a.full_size)
+    rows = ws.compare(model, range(5000, 5000 + a.heldout), R=a.rank, small=not a.full_size,
+                      family=a.family)
     rep = {
-        "train_tensors": a.count, "epochs": a.epochs, "lr": a.lr, "rank": a.rank, "hidden": a.hidden,
+        "train_tensors": a.count, "family": a.family, "epochs": a.epochs, "lr": a.lr, "rank": a.rank, "hidden": a.hidden,
         "label_gen_s": round(t1 - t0, 1), "train_s": round(t2 - t1, 1), "loss_history": hist,
         "heldout": rows,
         "mean_random_iters": float(np.mean([r["random_iters"] for r in rows])),

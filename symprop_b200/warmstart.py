@@ -94,10 +94,21 @@ def features(X: SpSymtensor, R: int, seed: int = 0):
     return out
 
 
-def random_tensor(seed: int, small: bool = True):
-    """A seeded training tensor: order in {3,4,5,6}, planted communities with
-    Zipf(1.2) degrees.  small=True shrinks n and nnz for quick training."""
+def random_tensor(seed: int, small: bool = True, family: str = "community"):
+    """A seeded training tensor.
+
+    family "community": order in {3,4,5,6}, planted communities with
+    Zipf(1.2) degrees (small=True shrinks n and nnz for quick training).
+    family "powerlaw": order 5, power-law degree weights (exponent 2.1) with
+    16 planted communities, 80% of the tuples inside one community, n in
+    [2000, 8000], 20k-200k tuples; a small version of the order-5 rank-16
+    learned-start workload."""
     rng = np.random.default_rng(10_000 + seed)
+    if family == "powerlaw":
+        n = int(rng.integers(2000, 8_001))
+        nnz = int(rng.integers(20_000, 200_001))
+        t = synth.powerlaw_communities(5, n, nnz, 2.1, 16, 0.8, 20_000 + seed)
+        return 5, n, t, np.ones(t.shape[0])
     order = int(rng.integers(3, 7))
     if small:
         n = int(rng.integers(1000, 4000))
@@ -110,11 +121,12 @@ def random_tensor(seed: int, small: bool = True):
     return order, n, t, np.ones(t.shape[0])
 
 
-def make_samples(seeds, R: int = 8, delta: float = 1.0, small: bool = True, log=print):
+def make_samples(seeds, R: int = 8, delta: float = 1.0, small: bool = True, log=print,
+                 family: str = "community"):
     import torch
     out = []
     for s in seeds:
-        order, n, t, v = random_tensor(s, small)
+        order, n, t, v = random_tensor(s, small, family)
         X = SpSymtensor(n, order, t, v)
         d = X.TuckerHOOI(rank=R, max_iter=200, rel_tol=1e-10, delta=delta, seed=s)
         Ut = torch.from_numpy(np.ascontiguousarray(d.factor)).cuda()
@@ -167,12 +179,12 @@ def train(model: WarmStartModel, samples, epochs: int = 20, lr: float = 1e-3, se
 
 
 def compare(model: WarmStartModel, seeds, R: int = 8, delta: float = 1.0, tol: float = 1e-6,
-            small: bool = True, precision: int = 0):
+            small: bool = True, precision: int = 0, family: str = "community"):
     """Random-start vs learned-start HOOI on held-out tensors: iterations,
     final errors and device time."""
     rows = []
     for s in seeds:
-        order, n, t, v = random_tensor(s, small)
+        order, n, t, v = random_tensor(s, small, family)
         X = SpSymtensor(n, order, t, v)
         base = X.TuckerHOOI(rank=R, max_iter=200, rel_tol=tol, delta=delta, seed=s, precision=precision)
         t0 = time.perf_counter()
