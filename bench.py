@@ -162,6 +162,19 @@ def load_traffic(precision):
     return None
 
 
+def max_over_ranks(x: float, device: str = "cuda") -> float:
+    """The largest x over the ranks of the default process group (x itself
+    when there is none): every timing of a multi-rank run is the slowest
+    rank's."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(x)
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def dist_env():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -299,11 +312,7 @@ def main():
             step()
         ev1.record(stream)
         torch.cuda.synchronize()
-    elapsed_ms = ev0.elapsed_time(ev1)
-    if ws > 1:
-        tt = torch.tensor([elapsed_ms], dtype=torch.float64, device="cuda")
-        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
-        elapsed_ms = float(tt.item())
+    elapsed_ms = max_over_ranks(ev0.elapsed_time(ev1))
     ms_step = elapsed_ms / args.steps
     value = ws * B / (ms_step * 1e-3) / 1e9
 
@@ -327,11 +336,7 @@ def main():
     te = time.perf_counter()
     for _ in range(args.e2e_steps):
         e2e_step()
-    e2e_ms = (time.perf_counter() - te) * 1e3 / args.e2e_steps
-    if ws > 1:
-        tt = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
-        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
-        e2e_ms = float(tt.item())
+    e2e_ms = max_over_ranks((time.perf_counter() - te) * 1e3 / args.e2e_steps)
     e2e_val = ws * B / (e2e_ms * 1e-3) / 1e9
     # result check against the device result of the timed loop
     diff = float((hY.cuda() - dY).abs().max().item())

@@ -71,6 +71,21 @@ int symprop_tensor_create(uint32_t order, uint32_t dim, const uint32_t *inds,
                           symprop_tensor **out);
 int symprop_tensor_destroy(symprop_tensor *t);
 
+/* Reads a .tns file and builds the tensor, parsing the text on the device.
+ * Replaces SymtensLoader::SymtensLoader (src/utils/loader.cpp:8-36) followed
+ * by SpSymtensor::SpSymtensor.  Same records as the loader: tuples sorted
+ * ascending; reading stops where the loader's stream stops (a trailing
+ * partial record, and a last value that ends the file with no whitespace
+ * after it, are dropped).  A malformed token (one the loader's stream would
+ * stop on or read only in part) gives SYMPROP_ERR_INVALID with its byte
+ * offset instead of a silently shortened tensor.  Orders 2..8. */
+int symprop_tensor_load_tns(const char *path, symprop_tensor **out);
+
+/* Copies the tensor's sorted tuples (nnz*order uint32, 1-based) and values
+ * (nnz) to host arrays; either pointer may be NULL.
+ * SpSymtensor::unnz_inds / unnzs (include/detail/sparse/spsymtensor.hpp:35-37). */
+int symprop_tensor_copy_nonzeros(const symprop_tensor *t, uint32_t *inds, double *vals);
+
 /* order/dim/size/norm accessors: include/detail/sparse/spsymtensor.hpp:29-34,43 */
 int symprop_tensor_order(const symprop_tensor *t, uint32_t *order);
 int symprop_tensor_dim(const symprop_tensor *t, uint32_t *dim);

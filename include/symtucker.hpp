@@ -169,6 +169,15 @@ class SpSymtensor {  // include/detail/sparse/spsymtensor.hpp:24-65
     std::cout << "Finished creating compressed dtree\n";  // spsymtensor.cpp:26
   }
 
+  // SymtensLoader + SpSymtensor in one step, with the .tns text parsed on
+  // the device (symprop_tensor_load_tns); same tensor as
+  // SpSymtensor(loader.dim(), loader.order(), loader.unnz_inds(), loader.unnzs())
+  static SpSymtensor load_tns(const std::string &path) {
+    symprop_tensor *t = nullptr;
+    check_status(symprop_tensor_load_tns(path.c_str(), &t));
+    return SpSymtensor(t);
+  }
+
   order_t order() const { return _order; }
   dim_t dim() const { return _dim; }
   index_t size() const { return _unnz; }
@@ -204,6 +213,19 @@ class SpSymtensor {  // include/detail/sparse/spsymtensor.hpp:24-65
   struct Del {
     void operator()(symprop_tensor *t) const { symprop_tensor_destroy(t); }
   };
+
+  explicit SpSymtensor(symprop_tensor *t) : _t(t) {
+    uint64_t nnz = 0;
+    check_status(symprop_tensor_order(t, &_order));
+    check_status(symprop_tensor_dim(t, &_dim));
+    check_status(symprop_tensor_nnz(t, &nnz));
+    _unnz = (index_t)nnz;
+    _unnz_inds.resize((size_t)nnz * _order);
+    _unnzs.resize((size_t)nnz);
+    check_status(symprop_tensor_copy_nonzeros(t, _unnz_inds.data(), _unnzs.data()));
+    check_status(symprop_tensor_norm(t, &_norm));
+    std::cout << "Finished creating compressed dtree\n";  // spsymtensor.cpp:26
+  }
 
   SymTuckerDecomp run(const Config &c, int alg) const {
     SymTuckerDecomp d(c, _dim, _order);

@@ -5,6 +5,8 @@
 //   ref_probe tree   <tensor.spt> <out.bin>                 CompressedDTree dump
 //   ref_probe s3ttmc <tensor.spt> <R> <U.f64> <packed> <Y.f64>
 //   ref_probe time   <tensor.spt> <R> <reps> <packed>       S3TTMc wall time
+//   ref_probe load   <tensor.tns> <out.bin>                 SymtensLoader result
+//                    (order u32, dim u32, nnz u64, ids, values) and its time
 //
 // <tensor.spt> is the binary tuple format written by symprop_b200 (magic
 // "SPT1", order, dim, nnz, nnz*order uint32 1-based sorted ids, nnz float64).
@@ -36,6 +38,7 @@
 #include <detail/compressed_dtree.hpp>
 #undef private
 #undef protected
+#include <utils/loader.hpp>
 #include <omp.h>
 
 using namespace symprop;
@@ -83,6 +86,25 @@ int main(int argc, char **argv) {
     return 1;
   }
   std::string mode = argv[1];
+  if (mode == "load" && argc >= 4) {
+    auto l0 = std::chrono::steady_clock::now();
+    SymtensLoader L(argv[2]);
+    auto l1 = std::chrono::steady_clock::now();
+    FILE *f = std::fopen(argv[3], "wb");
+    uint32_t order = L.order(), dim = L.dim();
+    uint64_t nnz = L.unnzs().size();
+    put(f, order);
+    put(f, dim);
+    put(f, nnz);
+    if (nnz) {
+      std::fwrite(L.unnz_inds().data(), sizeof(dim_t), L.unnz_inds().size(), f);
+      std::fwrite(L.unnzs().data(), sizeof(real_t), nnz, f);
+    }
+    std::fclose(f);
+    std::printf("{\"load_ms\": %.3f, \"nnz\": %llu}\n",
+                std::chrono::duration<double, std::milli>(l1 - l0).count(), (unsigned long long)nnz);
+    return 0;
+  }
   Tuples t = read_spt(argv[2]);
   auto t0 = std::chrono::steady_clock::now();
   SpSymtensor X(t.dim, t.order, t.inds, t.vals);

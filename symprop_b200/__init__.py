@@ -95,6 +95,8 @@ def lib():
         "symprop_gram_device": (_I, [_P, _U64, _U32, _P, _P, _I, _P]),
         "symprop_s3ttmc_schedule": (_I, [_I]),
         "symprop_gram_device_noalloc": (_I, [_P, _U64, _U32, _P, _P, _P]),
+        "symprop_tensor_load_tns": (_I, [ctypes.c_char_p, ctypes.POINTER(_P)]),
+        "symprop_tensor_copy_nonzeros": (_I, [_P, _P, _P]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -113,6 +115,7 @@ def exported_symbols() -> list[str]:
         "symprop_tree_copy_owners", "symprop_s3ttmc", "symprop_s3ttmc_device", "symprop_s3ttmc_launches",
         "symprop_symtens_size", "symprop_symtens_coeff", "symprop_unpack_rows_device", "symprop_tucker",
         "symprop_write_decomp", "symprop_gram_device", "symprop_s3ttmc_schedule",
+        "symprop_tensor_load_tns", "symprop_tensor_copy_nonzeros",
     ]
 
 
@@ -189,6 +192,30 @@ class SpSymtensor:
         n = _D(0)
         _check(lib().symprop_tensor_norm(self._h, ctypes.byref(n)))
         self._norm = n.value
+
+    @classmethod
+    def load_tns(cls, path: str) -> "SpSymtensor":
+        """SymtensLoader + SpSymtensor with the .tns text parsed on the device
+        (symprop_tensor_load_tns)."""
+        self = cls.__new__(cls)
+        h = _P()
+        _check(lib().symprop_tensor_load_tns(os.fsencode(path), ctypes.byref(h)))
+        self._h = h
+        o, d, z, n = _U32(0), _U32(0), _U64(0), _D(0)
+        _check(lib().symprop_tensor_order(h, ctypes.byref(o)))
+        _check(lib().symprop_tensor_dim(h, ctypes.byref(d)))
+        _check(lib().symprop_tensor_nnz(h, ctypes.byref(z)))
+        _check(lib().symprop_tensor_norm(h, ctypes.byref(n)))
+        self._order, self._dim, self._nnz, self._norm = o.value, d.value, z.value, n.value
+        return self
+
+    def nonzeros(self):
+        """(inds nnz x order uint32, vals nnz float64) as held on the device
+        (SpSymtensor::unnz_inds / unnzs)."""
+        inds = np.empty((self._nnz, self._order), dtype=np.uint32)
+        vals = np.empty(self._nnz, dtype=np.float64)
+        _check(lib().symprop_tensor_copy_nonzeros(self._h, _ptr(inds), _ptr(vals)))
+        return inds, vals
 
     def close(self):
         if getattr(self, "_h", None):

@@ -56,19 +56,27 @@ def main():
     ap.add_argument("--arms", default="fp64_random,mixed_random,mixed_learned,fp64_learned",
                     help="comma list of fp64_random, mixed_random, mixed_learned, fp64_learned")
     ap.add_argument("--no-warmup", action="store_true", help="skip the untimed first solve")
+    ap.add_argument("--alg", default="hooi", choices=["hooi", "hoqri"])
     a = ap.parse_args()
     arms = set(a.arms.split(","))
     order, n, t, v = synth.workload(a.workload, scale=a.scale)
     X = SpSymtensor(n, order, t, v)
     rows = []
+    ref64_box, solved = [], []
 
     def solve(name, precision, init="rnd", U0=None, extra_ms=0.0):
         kw = dict(rank=a.rank, max_iter=a.iters, rel_tol=a.tol, delta=a.delta, seed=0, precision=precision)
         if U0 is not None:
             kw.update(init="user", init_factor=U0)
-        d = X.TuckerHOOI(**kw)
+        d = (X.TuckerHOOI if a.alg == "hooi" else X.TuckerHOQRI)(**kw)
         row = {"arm": name, "iters": d.iterations, "error": d.error, "ms": d.time_ms + extra_ms,
                "s3ttmc_ms": d.s3ttmc_ms, "dense_ms": d.dense_ms}
+        if ref64_box:  # errors against the FP64 random-start solve (the oracle arm)
+            r64 = ref64_box[0]
+            sv = np.linalg.svd(r64.factor.T @ d.factor, compute_uv=False)
+            row["max_principal_angle_vs_fp64"] = float(np.arccos(np.clip(sv.min(), -1.0, 1.0)))
+            row["core_norm_sq_rel_err_vs_fp64"] = abs(d.core_norm ** 2 - r64.core_norm ** 2) / r64.core_norm ** 2
+        solved.append(d)
         rows.append(row)
         print(json.dumps(row))
         return d
@@ -77,6 +85,8 @@ def main():
         solve("warmup", PREC_FP64)  # first-use plans and module loading
         rows.clear()
     ref64 = solve("fp64_random", PREC_FP64) if "fp64_random" in arms else None
+    if ref64 is not None:
+        ref64_box.append(ref64)
     if "mixed_random" in arms:
         solve("mixed_random", PREC_MIXED)
     wpath = a.weights

@@ -459,6 +459,11 @@ __global__ void random_fill_kernel(double *A, size_t n, uint64_t seed) {
   A[i] = ((double)(z >> 11) * (1.0 / 9007199254740992.0)) - 0.5;
 }
 
+__global__ void eye_kernel(double *I, int s) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < s) I[(size_t)i * s + i] = 1.0;
+}
+
 __global__ void copy_cols_kernel(const double *src, int lds, int rows, int cols, double *dst,
                                  int ldd) {
   size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -654,12 +659,37 @@ static bool eig_trace() {
 // Block Krylov (block Lanczos with full re-orthogonalisation and thick
 // restart) for the top-r eigenpairs of S.  Projected problems of at most
 // kJacobiMax columns are solved by jacobi_eig.
+static int top_eigs_op(cudaStream_t st, const SymApply &apply, int s, int r, double *V, double *lam,
+                       const double *warm, double tol, int max_restarts, const double *dense);
+
 int top_eigs(cudaStream_t st, const double *S, int s, int r, double *V, double *lam,
              const double *warm, double tol, int max_restarts) {
+  SymApply apply = [S, s](cudaStream_t stream, const double *X, int ldx, int cols, double *Y, int ldy) {
+    gemm<double>(stream, s, cols, s, 1.0, S, s, false, X, ldx, false, 0.0, Y, ldy);
+  };
+  return top_eigs_op(st, apply, s, r, V, lam, warm, tol, max_restarts, S);
+}
+
+int top_eigs_op(cudaStream_t st, const SymApply &apply, int s, int r, double *V, double *lam,
+                const double *warm, double tol, int max_restarts) {
+  return top_eigs_op(st, apply, s, r, V, lam, warm, tol, max_restarts, nullptr);
+}
+
+// dense: the matrix itself when it is at hand (small s goes straight to Jacobi)
+static int top_eigs_op(cudaStream_t st, const SymApply &apply, int s, int r, double *V, double *lam,
+                const double *warm, double tol, int max_restarts, const double *dense) {
   if (r > s) fail(SYMPROP_ERR_INVALID, "rank %d exceeds matrix size %d", r, s);
   if (s <= kJacobiMax) {
-    Scratch w(sizeof(double) * s, st), Z(sizeof(double) * s * s, st);
-    jacobi_eig(st, S, s, w.as<double>(), Z.as<double>());
+    Scratch w(sizeof(double) * s, st), Z(sizeof(double) * s * s, st), Sd(dense ? 0 : sizeof(double) * s * s, st);
+    if (!dense) {  // form the small matrix: S = S I
+      Scratch I(sizeof(double) * s * s, st);
+      SPB_CUDA(cudaMemsetAsync(I.p, 0, sizeof(double) * s * s, st));
+      eye_kernel<<<cdiv(s, 256), 256, 0, st>>>(I.as<double>(), s);
+      SPB_LAUNCH_CHECK();
+      apply(st, I.as<double>(), s, s, Sd.as<double>(), s);
+      dense = Sd.as<double>();
+    }
+    jacobi_eig(st, dense, s, w.as<double>(), Z.as<double>());
     copy_cols_kernel<<<cdiv((long long)s * r, 256), 256, 0, st>>>(Z.as<double>(), s, s, r, V, r);
     SPB_LAUNCH_CHECK();
     SPB_CUDA(cudaMemcpyAsync(lam, w.p, sizeof(double) * r, cudaMemcpyDeviceToHost, st));
@@ -703,7 +733,7 @@ int top_eigs(cudaStream_t st, const double *S, int s, int r, double *V, double *
       // (column-scaled CholQR2; Householder when W is numerically rank
       // deficient, then a second projection removes any direction it
       // invented inside the existing basis).
-      gemm<double>(st, s, b, s, 1.0, S, s, false, q + (j - 1) * b, nb, false, 0.0, blk.as<double>(), b);
+      apply(st, q + (j - 1) * b, nb, b, blk.as<double>(), b);
       project_out(st, q, nb, width, blk.as<double>(), s, b, C.as<double>());
       if (orthonormalize(st, blk.as<double>(), s, b)) {
         project_out(st, q, nb, width, blk.as<double>(), s, b, C.as<double>());
@@ -715,7 +745,7 @@ int top_eigs(cudaStream_t st, const double *S, int s, int r, double *V, double *
       width += b;
     }
     // Rayleigh-Ritz: T = Q^T S Q
-    gemm<double>(st, s, nb, s, 1.0, S, s, false, q, nb, false, 0.0, sq, nb);
+    apply(st, q, nb, nb, sq, nb);
     gemm<double>(st, nb, nb, s, 1.0, q, nb, true, sq, nb, false, 0.0, T.as<double>(), nb);
     jacobi_eig(st, T.as<double>(), nb, w.as<double>(), Z.as<double>());
     // X = Q Z[:, :b], SX = SQ Z[:, :b]

@@ -5,6 +5,8 @@
 // CBLAS/LAPACKE calls of the reference (src/dense/matrixops.cpp:18-146).
 #pragma once
 
+#include <functional>
+
 #include "common.cuh"
 
 namespace spb {
@@ -43,6 +45,13 @@ void jacobi_eig(cudaStream_t st, const double *S, int n, double *w, double *V);
 // Returns SYMPROP_OK or SYMPROP_ERR_NOCONV.
 int top_eigs(cudaStream_t st, const double *S, int s, int r, double *V, double *lam,
              const double *warm, double tol, int max_restarts);
+
+// The same for a symmetric operator given by its action Y = S X on row-major
+// blocks (X: s x cols with leading dimension ldx, Y: s x cols, ldy), for
+// matrices that are never formed.
+using SymApply = std::function<void(cudaStream_t st, const double *X, int ldx, int cols, double *Y, int ldy)>;
+int top_eigs_op(cudaStream_t st, const SymApply &apply, int s, int r, double *V, double *lam,
+                const double *warm, double tol, int max_restarts);
 
 // elementwise helpers
 void scale_sym(cudaStream_t st, double *G, int m, const double *sd);  // G[i][j] *= sd[i] sd[j]

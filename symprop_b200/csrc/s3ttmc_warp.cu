@@ -63,6 +63,7 @@ struct WarpParams {
   uint32_t ndesc, desc_begin[kMaxL + 1], desc_count[kMaxL + 1];
   uint32_t lvl_off[kMaxL + 1];  // offset of the first level-d tensor in a staging area
   uint32_t m[kMaxL + 1], m4[kMaxL + 1];
+  uint32_t mstr[kMaxL + 1];  // element stride between the level-d tensors (FP64 row padding included)
   uint32_t pair_src[kMaxL * kMaxL];  // level N-3 tensor of the positions other than {k,t}
   const int4 *tiles;                 // per tile: (first row r0 inside block j, j, first column x0, 0)
   const uint4 *rowoff;               // per tile: lex offset - j of its 4 rows, or kPadRow
@@ -146,6 +147,15 @@ __host__ __device__ constexpr int nmasks(int L, int d) {
   return c;
 }
 
+// Storage position of row r of a level tensor.  FP64 inserts 2 doubles
+// after every 16 rows: the 4-row groups that lanes fetch with two 128-bit
+// loads then fall on distinct banks (row groups 128 bytes apart would
+// otherwise share them).  FP32 rows are unpadded (16-byte groups are
+// conflict-free).  The host sizes the tensors with level_stride().
+template <typename T> __device__ __forceinline__ uint32_t prow(uint32_t r) {
+  return sizeof(T) == 8 ? r + 2 * (r >> 4) : r;
+}
+
 template <int L, int M, int K, int NS, typename T>
 __device__ __forceinline__ void dp_term(T &v, const T (&src)[NS], const T (&uj)[L]) {
   if constexpr (((M >> K) & 1) != 0) {
@@ -160,7 +170,7 @@ __device__ __forceinline__ void dp_mask(T *dst, uint32_t stride, uint32_t e, con
   constexpr int M = mask_at(L, D, I);
   T v = T(0);
   (dp_term<L, M, K, NS, T>(v, src, uj), ...);
-  dst[(uint32_t)I * stride + e] = v;
+  dst[(uint32_t)I * stride + prow<T>(e)] = v;
 }
 
 template <int L, int D, int NS, typename T, int... I>
@@ -183,7 +193,7 @@ __device__ __forceinline__ void dp_level(const WarpParams &p, const SmemTables &
   const uint8_t *jt = tb.jt + p.jtab_off[D];
   const uint32_t *stt = tb.start + D * (p.R + 1);
   const T *srcK = sK + p.lvl_off[D - 1];
-  const uint32_t sstr = p.m4[D - 1];
+  const uint32_t sstr = p.mstr[D - 1];
   T *dst = sK + p.lvl_off[D];
   for (uint32_t e = tid; e < md; e += nthr) {
     const uint32_t j = jt[e], r = e - stt[j];
@@ -191,8 +201,8 @@ __device__ __forceinline__ void dp_level(const WarpParams &p, const SmemTables &
 #pragma unroll
     for (int k = 0; k < L; ++k) uj[k] = sU[k * R4 + j];
 #pragma unroll
-    for (int i = 0; i < NS; ++i) src[i] = (D == 2) ? sU[i * R4 + r] : srcK[i * sstr + r];
-    dp_masks<L, D, NS, T>(dst, p.m4[D], e, src, uj, std::make_integer_sequence<int, nmasks(L, D)>{});
+    for (int i = 0; i < NS; ++i) src[i] = (D == 2) ? sU[i * R4 + r] : srcK[i * sstr + prow<T>(r)];
+    dp_masks<L, D, NS, T>(dst, p.mstr[D], e, src, uj, std::make_integer_sequence<int, nmasks(L, D)>{});
   }
 }
 
@@ -242,7 +252,7 @@ __device__ __forceinline__ void tile_step(const WarpParams &p, const T *sU, cons
           const uint32_t s = p.pair_src[pidx(k, t, L)];
           T kv[4];
           if constexpr (L == 3) ld4(sU + (s & 0xffu) * R4 + r0, kv);
-          else ld4(sK + s + r0, kv);
+          else ld4(sK + s + prow<T>(r0), kv);
 #pragma unroll
           for (int q = 0; q < 4; ++q) {
             A[k][q] += kv[q] * uj[t];
@@ -559,7 +569,7 @@ struct WarpPlan {
   bool ok = false;
   uint32_t L = 0, R = 0, R4 = 0, NTL = 0;
   bool team = false;  // team kernel (4 warps per work item) instead of one warp
-  uint32_t m[kMaxL + 1] = {}, m4[kMaxL + 1] = {};
+  uint32_t m[kMaxL + 1] = {}, m4[kMaxL + 1] = {}, mstr[kMaxL + 1] = {};
   DBuf<uint32_t> starts;
   DBuf<uint8_t> jtab;
   uint32_t jtab_len = 0, jtab_off[kMaxL + 1] = {};
@@ -582,6 +592,9 @@ std::shared_ptr<WarpPlan> warp_plan(uint32_t N, uint32_t R) {
   for (uint32_t d = 0; d <= L; ++d) {
     pl->m[d] = (uint32_t)symsize(R, d);
     pl->m4[d] = (pl->m[d] + 3) / 4 * 4;
+    // covers prow<double>(m4 - 1); a multiple of 4 elements so that every
+    // tensor starts 16-byte aligned for the FP32 float4 and FP64 double2 loads
+    pl->mstr[d] = (pl->m4[d] + 2 * ((pl->m4[d] + 15) / 16) + 3) / 4 * 4;
   }
   if (pl->m[L - 1] >= (1u << 24)) return pl;
   std::vector<uint32_t> starts((size_t)(L + 1) * (R + 1), 0);
@@ -651,7 +664,7 @@ std::shared_ptr<WarpPlan> warp_plan(uint32_t N, uint32_t R) {
       WDesc ds{};
       ds.dst = ksz;
       offm[mask] = ksz;
-      ksz += pl->m4[d];
+      ksz += pl->mstr[d];
       for (uint32_t k = 0; k < L; ++k) {
         if (!(mask & (1u << k))) continue;
         uint32_t src = mask & ~(1u << k);
@@ -767,6 +780,7 @@ void warp_launch(const WarpPlan &pl, const TensorState &t, const void *dU, void 
     wp.lvl_off[d] = pl.lvl_off[d];
     wp.m[d] = pl.m[d];
     wp.m4[d] = pl.m4[d];
+    wp.mstr[d] = pl.mstr[d];
   }
   for (int i = 0; i < kMaxL * kMaxL; ++i) wp.pair_src[i] = pl.pair_src[i];
   wp.tiles = pl.tiles.p;

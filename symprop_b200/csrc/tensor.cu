@@ -128,7 +128,7 @@ inline unsigned grid_for(uint64_t n, unsigned block) {
 
 }  // namespace
 
-void tensor_build(TensorState &t, const uint32_t *h_inds, const double *h_vals) {
+void tensor_build(TensorState &t, const uint32_t *h_inds, const double *h_vals, bool on_device) {
   const uint32_t N = t.order;
   const uint64_t nnz = t.nnz;
   cudaStream_t st = 0;
@@ -138,8 +138,9 @@ void tensor_build(TensorState &t, const uint32_t *h_inds, const double *h_vals) 
   t.inds.alloc(nnz * N);
   t.vals.alloc(nnz);
   if (nnz) {
-    SPB_CUDA(cudaMemcpy(raw.p, h_inds, nnz * N * sizeof(uint32_t), cudaMemcpyHostToDevice));
-    SPB_CUDA(cudaMemcpy(t.vals.p, h_vals, nnz * sizeof(double), cudaMemcpyHostToDevice));
+    const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    SPB_CUDA(cudaMemcpy(raw.p, h_inds, nnz * N * sizeof(uint32_t), kind));
+    SPB_CUDA(cudaMemcpy(t.vals.p, h_vals, nnz * sizeof(double), kind));
   }
   DBuf<int> bad(1);
   SPB_CUDA(cudaMemset(bad.p, 0, sizeof(int)));

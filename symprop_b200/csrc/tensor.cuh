@@ -115,7 +115,8 @@ void unpack_rows(const void *dpacked, uint64_t rows, uint32_t dim, uint32_t orde
 // tree.cu
 void tree_build(TensorState &t);
 // tensor.cu
-void tensor_build(TensorState &t, const uint32_t *h_inds, const double *h_vals);
+// inds/vals in host memory, or in device memory when on_device is set
+void tensor_build(TensorState &t, const uint32_t *inds, const double *vals, bool on_device = false);
 
 }  // namespace spb
 
