@@ -25,7 +25,7 @@
 // x >= last(p), are consecutive in the reference's lexicographic packed
 // order, so a tile row is written at a precomputed row offset + x (no
 // permutation table).  FP32 mode folds the lane's plain FP32 sums into a
-// Kahan-compensated accumulator in shared memory every 8 owners.
+// Kahan-compensated accumulator in shared memory every 16 owners.
 #include <algorithm>
 #include <utility>
 
@@ -35,7 +35,7 @@ namespace spb {
 namespace {
 
 constexpr int kWarps = 4, kThreads = kWarps * 32, kMaxL = 7, kMaxNTL = 4;
-constexpr int kFold = 8;  // FP32: owners summed plainly between Kahan folds
+constexpr int kFold = 16;  // FP32: owners summed plainly between Kahan folds
 constexpr uint32_t kURow = 0x80000000u;
 constexpr uint32_t kPadRow = 0xffffffffu;
 
@@ -88,6 +88,10 @@ __host__ __device__ constexpr int pidx(int k, int t, int L) { return k * L + t; 
 template <typename T, int NTL> __host__ __device__ constexpr int min_blocks() {
   return sizeof(T) == 8 ? (NTL == 1 ? 4 : NTL <= 3 ? 3 : 2) : (NTL <= 3 ? 4 : 3);
 }
+
+// Team kernel: owners advanced per pipeline step (two halve the barriers;
+// order 6 and up keep one so the (order-1) x 2 staging buffers fit)
+__host__ __device__ constexpr int team_owners_per_step(int L) { return L <= 4 ? 2 : 1; }
 
 // U values of one owner staged per lane by the warp kernel (the plan checks
 // L * R4 <= 32 * kP)
@@ -467,14 +471,16 @@ __global__ void __launch_bounds__(kThreads, (min_blocks<T, NTL>())) s3ttmc_warp_
 template <int L, int NTL, typename T>
 __global__ void __launch_bounds__(kThreads, (min_blocks<T, NTL>())) s3ttmc_team_kernel(const WarpParams p) {
   constexpr bool kExact = sizeof(T) == 8;
-  constexpr int kD = L - 1;  // pipeline depth = buffers
+  constexpr int kD = L - 1;                // pipeline depth (steps)
+  constexpr int kOps = team_owners_per_step(L);  // owners per step (one barrier each)
+  constexpr int kNB = kOps * kD;           // staging buffers
   extern __shared__ __align__(16) unsigned char smem[];
   const uint32_t tid = threadIdx.x;
   const uint32_t R = p.R, R4 = p.R4, LR4 = (uint32_t)L * R4;
 
   const SmemTables tb = load_tables<L>(p, smem, (int)tid, kThreads);
-  T *sBuf = reinterpret_cast<T *>(tb.rest);  // kD x wsz
-  float2 *sK2 = reinterpret_cast<float2 *>(sBuf + (size_t)kD * p.wsz);
+  T *sBuf = reinterpret_cast<T *>(tb.rest);  // kNB x wsz
+  float2 *sK2 = reinterpret_cast<float2 *>(sBuf + (size_t)kNB * p.wsz);
   const Chunk ch = p.chunks[blockIdx.x];
 
   int4 tl[NTL];
@@ -499,58 +505,74 @@ __global__ void __launch_bounds__(kThreads, (min_blocks<T, NTL>())) s3ttmc_team_
   }
   // the padding rows of the level tensors are read (and discarded) by the
   // last level: keep them finite
-  for (uint32_t i = tid; i < (uint32_t)kD * p.wsz; i += kThreads) sBuf[i] = T(0);
+  for (uint32_t i = tid; i < (uint32_t)kNB * p.wsz; i += kThreads) sBuf[i] = T(0);
   __syncthreads();
 
   const T *U = reinterpret_cast<const T *>(p.U);
   const T *own_c = reinterpret_cast<const T *>(p.own_c);
   const uint64_t nown = ch.oe - ch.ob;
-  // staging thread tid < L*R4 owns element (k, x) of every owner; the U
-  // value and coefficient of the next owner and the id of the one after
-  // are loaded one step ahead
-  const bool stager = tid < LR4;
-  const uint32_t sk = stager ? tid / R4 : 0u, sx = stager ? tid - sk * R4 : 0u;
+  auto buf = [&](uint64_t o) { return sBuf + (size_t)(o % kNB) * p.wsz; };
+  // staging thread tid < kOps*L*R4 owns element (k, x) of owner q of every
+  // step; the U value and coefficient of its next owner and the ids of the
+  // one after are loaded one step ahead
+  const bool stager = tid < (uint32_t)kOps * LR4;
+  const uint32_t sq = stager ? tid / LR4 : 0u, se = stager ? tid - sq * LR4 : 0u;
+  const uint32_t sk = se / R4, sx = se - sk * R4;
   auto load_id = [&](uint64_t o) -> uint32_t {
     return (stager && o < nown) ? p.own_S[(ch.ob + o) * p.sstride + sk] : 0u;
   };
   T u_n = T(0), c_n = T(0);
-  if (nown) {
-    const uint32_t id0 = load_id(0);
-    if (stager && sx < R) u_n = U[(uint64_t)id0 * R + sx];
-    c_n = own_c[ch.ob];
+  if (stager && sq < nown) {
+    const uint32_t id0 = load_id(sq);
+    if (sx < R) u_n = U[(uint64_t)id0 * R + sx];
+    c_n = own_c[ch.ob + sq];
   }
-  uint32_t id_n = load_id(1);
+  uint32_t id_n = load_id(kOps + sq);
   int pending = 0;
+  const uint64_t nsteps = (nown + kOps - 1) / kOps;
 
-  for (uint64_t s = 0; s < nown + kD - 1; ++s) {
-    if (s < nown) {  // stage owner s into buffer s % kD
-      T *b = sBuf + (size_t)(s % kD) * p.wsz;
-      if (stager) {
-        b[tid] = u_n;
-        b[LR4 + tid] = c_n * u_n;
+  for (uint64_t s = 0; s < nsteps + kD - 1; ++s) {
+    if (s < nsteps) {  // stage owners s*kOps .. s*kOps+kOps-1
+      const uint64_t o = s * kOps + sq;
+      if (stager && o < nown) {
+        T *b = buf(o);
+        b[se] = u_n;
+        b[LR4 + se] = c_n * u_n;
       }
-      if (s + 1 < nown) {
-        u_n = (stager && sx < R) ? U[(uint64_t)id_n * R + sx] : T(0);
-        c_n = own_c[ch.ob + s + 1];
+      const uint64_t on = o + kOps;
+      u_n = T(0);
+      if (stager && on < nown) {
+        if (sx < R) u_n = U[(uint64_t)id_n * R + sx];
+        c_n = own_c[ch.ob + on];
       }
-      id_n = load_id(s + 2);
+      id_n = load_id(on + kOps);
     }
     if constexpr (L >= 4) {
 #pragma unroll 1
-      for (int d = 2; d <= L - 2; ++d) {  // level d of owner s - (d - 1)
-        if (s >= (uint64_t)(d - 1) && s - (d - 1) < nown) {
-          T *b = sBuf + (size_t)((s - (d - 1)) % kD) * p.wsz;
-          dp_level_rt<L, T>(d, p, tb, b, b + 2 * LR4, tid, kThreads);
+      for (int d = 2; d <= L - 2; ++d) {  // level d of the owners staged d-1 steps ago
+        if (s < (uint64_t)(d - 1)) continue;
+#pragma unroll
+        for (int q = 0; q < kOps; ++q) {
+          const uint64_t o = (s - (d - 1)) * kOps + q;
+          if (o < nown) {
+            T *b = buf(o);
+            dp_level_rt<L, T>(d, p, tb, b, b + 2 * LR4, tid, kThreads);
+          }
         }
       }
     }
-    if (s >= (uint64_t)(kD - 1)) {  // tiles of owner s - (kD - 1)
-      const T *b = sBuf + (size_t)((s - (kD - 1)) % kD) * p.wsz;
-      tile_step<L, NTL, T>(p, b, b + LR4, b + 2 * LR4, tl, live, acc);
-      if constexpr (!kExact) {
-        if (++pending == kFold) {
-          pending = 0;
-          kahan_fold<NTL, T>(sK2, (uint32_t)kThreads, tid, acc);
+    if (s >= (uint64_t)(kD - 1)) {  // tiles of the owners staged kD-1 steps ago
+#pragma unroll
+      for (int q = 0; q < kOps; ++q) {
+        const uint64_t o = (s - (kD - 1)) * kOps + q;
+        if (o >= nown) break;
+        const T *b = buf(o);
+        tile_step<L, NTL, T>(p, b, b + LR4, b + 2 * LR4, tl, live, acc);
+        if constexpr (!kExact) {
+          if (++pending == kFold) {
+            pending = 0;
+            kahan_fold<NTL, T>(sK2, (uint32_t)kThreads, tid, acc);
+          }
         }
       }
     }
@@ -643,7 +665,7 @@ std::shared_ptr<WarpPlan> warp_plan(uint32_t N, uint32_t R) {
   // staging: the warp kernel stages stage_per_lane<L>() values per lane,
   // the team kernel one per thread
   if (!pl->team && L * pl->R4 > (L <= 2 ? 128u : 64u)) return pl;
-  if (pl->team && L * pl->R4 > (uint32_t)kThreads) return pl;
+  if (pl->team && (uint32_t)team_owners_per_step((int)L) * L * pl->R4 > (uint32_t)kThreads) return pl;
   // jtab and descriptors for levels 2..L-2
   std::vector<uint8_t> jt;
   for (uint32_t d = 2; d + 2 <= L; ++d) {
@@ -695,7 +717,7 @@ std::shared_ptr<WarpPlan> warp_plan(uint32_t N, uint32_t R) {
                    ((size_t)pl->ndesc * sizeof(WDesc) + 15) / 16 * 16;
     // warp kernel: one staging area per warp; team kernel: one per
     // pipeline stage (L-1); FP32 adds the Kahan pairs of every thread
-    size_t work = (size_t)(pl->team ? L - 1 : kWarps) * pl->wsz * es;
+    size_t work = (size_t)(pl->team ? (L - 1) * team_owners_per_step((int)L) : kWarps) * pl->wsz * es;
     if (pi == 1) work = (work + 15) / 16 * 16 + (size_t)kThreads * pl->NTL * 16 * sizeof(float) * 2;
     pl->smem[pi] = fixed + work;
     if (pl->smem[pi] > 200 * 1024) return pl;
