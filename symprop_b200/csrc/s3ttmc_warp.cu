@@ -83,6 +83,19 @@ template <typename T> __device__ __forceinline__ void ld4(const T *p, T (&v)[4])
 
 __host__ __device__ constexpr int pidx(int k, int t, int L) { return k * L + t; }  // k < t
 
+// (d0, d1) += (a0, a1) * (b0, b1) in one paired FP32 FMA (fma.rn.f32x2,
+// sm_100): each lane rounds exactly as a scalar fmaf does
+template <typename T>
+__device__ __forceinline__ void ffma2(T &d0, T &d1, T a0, T a1, T b0, T b1) {
+  static_assert(sizeof(T) == 4, "paired FMA is FP32");
+  unsigned long long d, a, b;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(d) : "f"(d0), "f"(d1));
+  asm("mov.b64 %0, {%1, %2};" : "=l"(a) : "f"(a0), "f"(a1));
+  asm("mov.b64 %0, {%1, %2};" : "=l"(b) : "f"(b0), "f"(b1));
+  asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(d) : "l"(a), "l"(b));
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(d0), "=f"(d1) : "l"(d));
+}
+
 // CTAs per SM the register budget is sized for (accumulators: NTL x 16
 // values per lane)
 template <typename T, int NTL> __host__ __device__ constexpr int min_blocks() {
@@ -257,22 +270,40 @@ __device__ __forceinline__ void tile_step(const WarpParams &p, const T *sU, cons
           T kv[4];
           if constexpr (L == 3) ld4(sU + (s & 0xffu) * R4 + r0, kv);
           else ld4(sK + s + prow<T>(r0), kv);
+          if constexpr (sizeof(T) == 4) {  // row pairs on the paired FP32 pipe
 #pragma unroll
-          for (int q = 0; q < 4; ++q) {
-            A[k][q] += kv[q] * uj[t];
-            A[t][q] += kv[q] * uj[k];
+            for (int h = 0; h < 4; h += 2) {
+              ffma2(A[k][h], A[k][h + 1], kv[h], kv[h + 1], uj[t], uj[t]);
+              ffma2(A[t][h], A[t][h + 1], kv[h], kv[h + 1], uj[k], uj[k]);
+            }
+          } else {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+              A[k][q] += kv[q] * uj[t];
+              A[t][q] += kv[q] * uj[k];
+            }
           }
         }
     }
+    if constexpr (sizeof(T) == 4) {
 #pragma unroll
-    for (int q = 0; q < 4; ++q)
+      for (int cc = 0; cc < 4; ++cc)
 #pragma unroll
-      for (int cc = 0; cc < 4; ++cc) {
-        T s = acc[i][q][cc];
+        for (int h = 0; h < 4; h += 2)
 #pragma unroll
-        for (int k = 0; k < L; ++k) s += A[k][q] * w[k][cc];
-        acc[i][q][cc] = s;
-      }
+          for (int k = 0; k < L; ++k)
+            ffma2(acc[i][h][cc], acc[i][h + 1][cc], A[k][h], A[k][h + 1], w[k][cc], w[k][cc]);
+    } else {
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+#pragma unroll
+        for (int cc = 0; cc < 4; ++cc) {
+          T s = acc[i][q][cc];
+#pragma unroll
+          for (int k = 0; k < L; ++k) s += A[k][q] * w[k][cc];
+          acc[i][q][cc] = s;
+        }
+    }
   }
 }
 
