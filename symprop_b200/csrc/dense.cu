@@ -10,6 +10,8 @@
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
+#include <map>
+#include <mutex>
 #include <vector>
 
 #include "dense.cuh"
@@ -491,11 +493,36 @@ __global__ void residual_kernel(const double *SX, const double *X, int s, int ld
   if (threadIdx.x == 0) res[i] = sqrt(red[0]);
 }
 
+// Stream-ordered scratch from a pool private to this library, one per
+// device, that keeps its memory between calls (release threshold: never):
+// the eigensolver's many small buffers then cost no allocation after the
+// first iteration.  (The device's default pool releases memory at every
+// synchronisation unless its owner raised the threshold.)
+cudaMemPool_t scratch_pool() {
+  static std::mutex mu;
+  static std::map<int, cudaMemPool_t> pools;
+  int dev = 0;
+  SPB_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(mu);
+  auto it = pools.find(dev);
+  if (it != pools.end()) return it->second;
+  cudaMemPoolProps props{};
+  props.allocType = cudaMemAllocationTypePinned;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = dev;
+  cudaMemPool_t pool;
+  SPB_CUDA(cudaMemPoolCreate(&pool, &props));
+  uint64_t keep = ~0ull;
+  SPB_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+  pools[dev] = pool;
+  return pool;
+}
+
 struct Scratch {
   void *p = nullptr;
   cudaStream_t st = 0;
   Scratch(size_t bytes, cudaStream_t s) : st(s) {
-    if (bytes) SPB_CUDA(cudaMallocAsync(&p, bytes, st));
+    if (bytes) SPB_CUDA(cudaMallocFromPoolAsync(&p, bytes, scratch_pool(), st));
   }
   ~Scratch() {
     if (p) cudaFreeAsync(p, st);

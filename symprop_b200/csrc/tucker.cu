@@ -23,6 +23,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdio>
 #include <cstdlib>
 #include <iomanip>
 #include <iostream>
@@ -204,6 +205,10 @@ int run_tucker(TensorState &t, const symprop_config &c, int alg, symprop_result 
 
   double prev_error = 0.0, error = 0.0, cn2 = 0.0;
   double s3_ms = 0, dense_ms = 0;
+  // SPB_TRACE_TUCKER=1 prints each iteration's precision, phase times and error
+  const char *tr = std::getenv("SPB_TRACE_TUCKER");
+  const bool trace = tr && *tr && *tr != '0';
+  double s3_prev = 0, dense_prev = 0;
   uint64_t iters = 0;
   int status = SYMPROP_OK;
   const int prec_digits = alg == SYMPROP_ALTHOOI ? 10 : 12;
@@ -314,6 +319,12 @@ int run_tucker(TensorState &t, const symprop_config &c, int alg, symprop_result 
     }
 
     error = std::sqrt(normX * normX - cn2) / normX;
+    if (trace) {
+      std::fprintf(stderr, "tucker: iter %llu %s s3ttmc %.1f ms dense %.1f ms error %.12e\n",
+                   (unsigned long long)iter, mx ? "mixed" : "fp64", s3_ms - s3_prev, dense_ms - dense_prev, error);
+      s3_prev = s3_ms;
+      dense_prev = dense_ms;
+    }
     if (iter < res.trace_cap) {
       if (res.error_trace) res.error_trace[iter] = error;
       if (res.relres_trace) res.relres_trace[iter] = rel_res;
