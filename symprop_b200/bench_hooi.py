@@ -71,6 +71,8 @@ def main():
         d = (X.TuckerHOOI if a.alg == "hooi" else X.TuckerHOQRI)(**kw)
         row = {"arm": name, "iters": d.iterations, "error": d.error, "ms": d.time_ms + extra_ms,
                "s3ttmc_ms": d.s3ttmc_ms, "dense_ms": d.dense_ms}
+        if extra_ms:
+            row["prediction_ms"] = extra_ms
         if ref64_box:  # errors against the FP64 random-start solve (the oracle arm)
             r64 = ref64_box[0]
             sv = np.linalg.svd(r64.factor.T @ d.factor, compute_uv=False)

@@ -213,6 +213,9 @@ int run_tucker(TensorState &t, const symprop_config &c, int alg, symprop_result 
   int status = SYMPROP_OK;
   const int prec_digits = alg == SYMPROP_ALTHOOI ? 10 : 12;
 
+  if (trace)
+    std::fprintf(stderr, "tucker: setup %.1f ms (buffers, init)\n",
+                 std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - wall0).count());
   for (uint64_t iter = 0; iter < c.max_iter; ++iter) {
     // eigen-residual target relative to the largest eigenvalue: the FP32 /
     // split-BF16 Gram of the mixed phase resolves about 1e-6 of it
