@@ -472,12 +472,12 @@ void s3ttmc_run(TensorState &t, const void *dU, uint32_t R, bool packed, void *d
   if (sched == kScheduleAuto || sched == kScheduleWarp) {
     auto it = t.warp.find(R);
     if (it == t.warp.end()) it = t.warp.emplace(R, warp_plan(t.order, R)).first;
-    if (warp_supported(*it->second) && (sched == kScheduleWarp || warp_preferred(*it->second))) {
+    if (warp_supported(*it->second)) {
       warp_launch(*it->second, t, dU, Ypk, precision, st);
       finish_rows(t, m, Ypk, packed, dY, R, L, precision, st);
       return;
     }
-    if (sched == kScheduleWarp && !warp_supported(*it->second))
+    if (sched == kScheduleWarp)
       fail(SYMPROP_ERR_SIZE, "warp S3TTMc does not support order %u rank %u", t.order, R);
   }
   if (sched == kScheduleAuto || sched == kScheduleTiled) {

@@ -1,31 +1,34 @@
-// S3TTMc, warp-per-owner schedule (the default for orders 3..5 when the
-// staged U rows fit two values per lane, e.g. order 4 / R <= 16, order 5 /
-// R <= 16).
+// S3TTMc, the default schedules: one warp per work item while a row's
+// 4 x 4 output tiles fit 3 per lane (order 4 / R <= 16, order 5 / R <= 8,
+// ...), otherwise a team of the CTA's 4 warps per work item (order 5 /
+// R = 16, order 6 / R = 10, ...).
 //
 // Same mathematics as the reference's level sweep
 // (CompressedDTree::kronecker_product_opt5, src/compressed_dtree.cpp:421-518;
 // SymOuterProd, include/detail/dense/symtensor.hpp:24-39):
 //     Y[i] += c * K(S),  K(S) = sum_k K(S \ s_k) (x) U[s_k].
-// A warp streams the owners (tree leaves) of one work item, one leaf per
-// step, with no CTA barrier inside the loop:
-//   * lanes stage the leaf's N-1 U rows (and c * U rows) in warp-private
-//     shared memory; the rows of the next leaf are loaded while the current
-//     one is computed;
-//   * levels 2..N-3 of the recursion are built in warp-private shared memory
-//     (colexicographic order, see s3ttmc_tiled.cu);
+// The owners (tree leaves) of a work item are streamed one leaf at a time:
+//   * the leaf's N-1 U rows (and c * U rows) are staged in shared memory;
+//     the rows of the next leaf are loaded while the current one is
+//     computed;
+//   * levels 2..N-3 of the recursion are built in shared memory
+//     (colexicographic order, see s3ttmc_tiled.cu), one element of all
+//     C(N-1, d) tensors of a level per thread, the sub-multisets enumerated
+//     at compile time;
 //   * the last level is never stored: for each of its 4 x 4 output tiles a
-//     lane evaluates the N-1 parent tensors K(S \ s_k) at the tile's 4 rows
-//     from level N-3 and U in registers, then adds the rank-(N-1) product
-//     with the c * U rows.
-// The output tiles of a row are split over G warps (NTL tiles per lane), so
-// the accumulators stay in registers whatever the packed row length; each of
-// the G warps streams the same owners.  A work item is a row, or a slice of
-// at most 256 owners of a long row whose FP64 partial sums a second kernel
-// adds in a fixed order.  For a fixed prefix p the outputs (p, x),
-// x >= last(p), are consecutive in the reference's lexicographic packed
-// order, so a tile row is written at a precomputed row offset + x (no
-// permutation table).  FP32 mode folds the lane's plain FP32 sums into a
-// Kahan-compensated accumulator in shared memory every 16 owners.
+//     thread evaluates the N-1 parent tensors K(S \ s_k) at the tile's 4
+//     rows from level N-3 and U in registers, then adds the rank-(N-1)
+//     product with the c * U rows.
+// Warp kernel: no CTA barrier in the owner loop.  Team kernel: the staging
+// and the levels are computed once for the 4 warps, in an (N-2)-deep
+// pipeline with one barrier per step (two leaves per step up to order 5).
+// A work item is a row, or a slice of at most 256 owners of a long row whose
+// FP64 partial sums a second kernel adds in a fixed order.  For a fixed
+// prefix p the outputs (p, x), x >= last(p), are consecutive in the
+// reference's lexicographic packed order, so a tile row is written at a
+// precomputed row offset + x (no permutation table).  FP32 tiles run on the
+// paired FMA (fma.rn.f32x2) and each thread folds its plain FP32 sums into
+// Kahan pairs in shared memory every 16 owners.
 #include <algorithm>
 #include <utility>
 
@@ -769,7 +772,6 @@ std::shared_ptr<WarpPlan> warp_plan(uint32_t N, uint32_t R) {
 }
 
 bool warp_supported(const WarpPlan &pl) { return pl.ok; }
-bool warp_preferred(const WarpPlan &pl) { return pl.ok; }
 
 template <int L, int NTL, typename T>
 static void launch_w(bool team, const WarpParams &wp, uint32_t nchunks, size_t smem, cudaStream_t st) {

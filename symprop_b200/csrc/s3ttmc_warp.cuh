@@ -1,4 +1,4 @@
-// Warp-per-owner S3TTMc schedule (s3ttmc_warp.cu).
+// Warp and team S3TTMc schedules (s3ttmc_warp.cu).
 #pragma once
 
 #include <memory>
@@ -10,8 +10,6 @@ namespace spb {
 struct WarpPlan;
 std::shared_ptr<WarpPlan> warp_plan(uint32_t N, uint32_t R);
 bool warp_supported(const WarpPlan &pl);
-// one warp per work item (the automatic schedule takes the warp kernel then)
-bool warp_preferred(const WarpPlan &pl);
 void warp_launch(const WarpPlan &pl, const TensorState &t, const void *dU, void *dYpacked,
                  int precision, cudaStream_t st);
 
