@@ -152,11 +152,11 @@ def load_peaks():
     return 6650.0, "fallback"
 
 
-def load_traffic(precision):
+def load_traffic(precision, workload, scale):
     """DRAM bytes per launch of the dominant kernel from the committed ncu
-    summary (profiles/), or None."""
-    p = os.path.join(ROOT, "profiles", "s3ttmc_order4_zipf_traffic.json")
-    if os.path.exists(p):
+    summary (profiles/) of this workload at full size, or None."""
+    p = os.path.join(ROOT, "profiles", f"{workload}_traffic.json")
+    if scale == 1.0 and os.path.exists(p):
         d = json.load(open(p))
         return d.get(precision)
     return None
@@ -343,7 +343,7 @@ def main():
 
     peak, peak_kind = load_peaks()
     achieved = B / (ms_step * 1e-3) / 1e9
-    traffic = load_traffic(args.precision)
+    traffic = load_traffic(args.precision, WORKLOAD, args.scale)
     clocks = clk.summary()
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline and WORKLOAD == "s3ttmc_order4_zipf":
@@ -359,8 +359,10 @@ def main():
                                    f"Y packed n x {m}", "parallelism": f"replicas x{ws}",
                        "levels": levels, "owners_after_merge": X.owner_count(),
                        "alg_bytes_per_step": B, "alg_flops_per_step": F,
-                       "l2": "inputs larger than L2 (owner list ~0.5 GB, Y %.2f GB); U (%.1f MB) is "
-                             "L2-resident within a step by design" % (n * m * s / 1e9, n * RANK * s / 1e6),
+                       "l2": "inputs larger than L2 (owner list %.2f GB, Y %.2f GB); U (%.1f MB) is "
+                             "L2-resident within a step by design"
+                             % (X.owner_count() * (4 * (-(-(order - 1) // 4) * 4) + s) / 1e9, n * m * s / 1e9,
+                                n * RANK * s / 1e6),
                        "build_ms": round(build_ms, 1)},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "traffic": traffic,

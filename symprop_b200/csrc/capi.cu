@@ -186,16 +186,7 @@ int symprop_s3ttmc(const symprop_tensor *t, const void *U, uint32_t R, int packe
     require(precision == SYMPROP_FP64 || precision == SYMPROP_FP32, "unknown precision");
     TensorState &s = const_cast<TensorState &>(t->s);
     set_current_device(s);
-    const size_t es = precision == SYMPROP_FP64 ? 8 : 4;
-    uint64_t cols = packed ? symsize(R, s.order - 1) : 1;
-    if (!packed)
-      for (uint32_t j = 0; j + 1 < s.order; ++j) cols *= R;
-    const size_t ubytes = (size_t)s.dim * R * es, ybytes = (size_t)s.dim * cols * es;
-    s.io_U.ensure(ubytes);
-    s.io_Y.ensure(ybytes);
-    SPB_CUDA(cudaMemcpy(s.io_U.p, U, ubytes, cudaMemcpyHostToDevice));
-    s3ttmc_run(s, s.io_U.p, R, packed != 0, s.io_Y.p, precision, 0);
-    SPB_CUDA(cudaMemcpy(Y, s.io_Y.p, ybytes, cudaMemcpyDeviceToHost));
+    s3ttmc_host(s, U, R, packed != 0, Y, precision);
   });
 }
 

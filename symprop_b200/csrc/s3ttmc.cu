@@ -19,7 +19,10 @@
 //    batches into a Kahan-compensated accumulator.
 #include <algorithm>
 #include <atomic>
+#include <cstdio>
 #include <cstdlib>
+#include <map>
+#include <mutex>
 
 #include "s3ttmc_tiled.cuh"
 #include "s3ttmc_warp.cuh"
@@ -27,8 +30,8 @@
 
 namespace spb {
 
-static void finish_rows(TensorState &t, uint64_t m, void *Ypk, bool packed, void *dY, uint32_t R,
-                        uint32_t L, int precision, cudaStream_t st);
+static void finish_rows(TensorState &t, const ItemSet &items, uint64_t m, void *Ypk, bool packed, void *dY,
+                        uint32_t R, uint32_t L, int precision, cudaStream_t st);
 
 static constexpr int kMaxL = 7;          // orders 2..8
 static constexpr uint32_t kURow = 0x80000000u;
@@ -445,36 +448,32 @@ void unpack_rows(const void *dpacked, uint64_t rows, uint32_t dim, uint32_t orde
   SPB_LAUNCH_CHECK();
 }
 
-void s3ttmc_run(TensorState &t, const void *dU, uint32_t R, bool packed, void *dY, int precision,
-                cudaStream_t st) {
-  if (R == 0) fail(SYMPROP_ERR_INVALID, "R must be positive");
-  if (precision != SYMPROP_FP64 && precision != SYMPROP_FP32)
-    fail(SYMPROP_ERR_INVALID, "unknown precision %d", precision);
+// One pass over a set of work items: writes the packed rows (or, when
+// `packed` is false, the full rows) [items.row0, items.row0 + items.rows) of
+// dY.  t.partials and t.scratch must already be large enough.
+static void s3ttmc_items(TensorState &t, const ItemSet &items, const void *dU, uint32_t R, bool packed,
+                         void *dY, int precision, cudaStream_t st) {
   const size_t es = precision == SYMPROP_FP64 ? 8 : 4;
   const uint32_t L = t.order - 1;
-  uint64_t m = symsize(R, L);
+  const uint64_t m = symsize(R, L);
   uint64_t full = 1;
   for (uint32_t j = 0; j < L; ++j) full *= R;
   const uint64_t ldy = packed ? m : full;
   if (t.order == 2) {
     // The reference's level loop is empty for depth 1 and Y stays zero
     // (src/compressed_dtree.cpp:451).
-    SPB_CUDA(cudaMemsetAsync(dY, 0, (size_t)t.dim * ldy * es, st));
+    if (items.rows)
+      SPB_CUDA(cudaMemsetAsync((char *)dY + (size_t)items.row0 * ldy * es, 0, (size_t)items.rows * ldy * es, st));
     return;
   }
-  void *Ypk = dY;
-  if (!packed) {
-    t.scratch.ensure((size_t)t.dim * m * es);
-    Ypk = t.scratch.p;
-  }
-  if (t.nslots) t.partials.ensure((size_t)t.nslots * m);
+  void *Ypk = packed ? dY : (void *)t.scratch.p;
   const int sched = s3ttmc_schedule();
   if (sched == kScheduleAuto || sched == kScheduleWarp) {
     auto it = t.warp.find(R);
     if (it == t.warp.end()) it = t.warp.emplace(R, warp_plan(t.order, R)).first;
     if (warp_supported(*it->second)) {
-      warp_launch(*it->second, t, dU, Ypk, precision, st);
-      finish_rows(t, m, Ypk, packed, dY, R, L, precision, st);
+      warp_launch(*it->second, t, items, dU, Ypk, precision, st);
+      finish_rows(t, items, m, Ypk, packed, dY, R, L, precision, st);
       return;
     }
     if (sched == kScheduleWarp)
@@ -484,8 +483,8 @@ void s3ttmc_run(TensorState &t, const void *dU, uint32_t R, bool packed, void *d
     auto it = t.tiled.find(R);
     if (it == t.tiled.end()) it = t.tiled.emplace(R, tiled_plan(t.order, R)).first;
     if (tiled_supported(*it->second)) {
-      tiled_launch(*it->second, t, dU, Ypk, precision, st);
-      finish_rows(t, m, Ypk, packed, dY, R, L, precision, st);
+      tiled_launch(*it->second, t, items, dU, Ypk, precision, st);
+      finish_rows(t, items, m, Ypk, packed, dY, R, L, precision, st);
       return;
     }
     if (sched == kScheduleTiled)
@@ -494,7 +493,7 @@ void s3ttmc_run(TensorState &t, const void *dU, uint32_t R, bool packed, void *d
   PackedTables &tb = tables_for(t, R);
 
   RowParams rp{};
-  rp.chunks = t.chunks.p;
+  rp.chunks = items.chunks;
   rp.own_S = t.own_S.p;
   rp.own_c = precision == SYMPROP_FP64 ? (const void *)t.own_c64.p : (const void *)t.own_c32.p;
   rp.sstride = t.sstride;
@@ -519,27 +518,162 @@ void s3ttmc_run(TensorState &t, const void *dU, uint32_t R, bool packed, void *d
   const size_t smem = tb.smem_bytes[precision == SYMPROP_FP64 ? 0 : 1];
   if (smem > 227 * 1024)
     fail(SYMPROP_ERR_SIZE, "order %u rank %u needs %zu bytes of shared memory", t.order, R, smem);
-  if (t.nchunks) {
+  if (items.nchunks) {
     if (precision == SYMPROP_FP64)
-      dispatch_rows<double>(L, tb, rp, t.nchunks, smem, st);
+      dispatch_rows<double>(L, tb, rp, items.nchunks, smem, st);
     else
-      dispatch_rows<float>(L, tb, rp, t.nchunks, smem, st);
+      dispatch_rows<float>(L, tb, rp, items.nchunks, smem, st);
   }
-  finish_rows(t, m, Ypk, packed, dY, R, L, precision, st);
+  finish_rows(t, items, m, Ypk, packed, dY, R, L, precision, st);
 }
 
-// combine the partial rows of split rows; unpack if requested
-static void finish_rows(TensorState &t, uint64_t m, void *Ypk, bool packed, void *dY, uint32_t R,
-                        uint32_t L, int precision, cudaStream_t st) {
-  if (t.nsplit) {
-    dim3 grid(t.nsplit, (unsigned)((m + 31) / 32));
+// make room for the partial sums of split rows and, for full output, the
+// packed staging rows
+static void s3ttmc_reserve(TensorState &t, uint32_t R, bool packed, int precision) {
+  if (R == 0) fail(SYMPROP_ERR_INVALID, "R must be positive");
+  if (precision != SYMPROP_FP64 && precision != SYMPROP_FP32)
+    fail(SYMPROP_ERR_INVALID, "unknown precision %d", precision);
+  const size_t es = precision == SYMPROP_FP64 ? 8 : 4;
+  const uint64_t m = symsize(R, t.order - 1);
+  if (!packed && t.order > 2) t.scratch.ensure((size_t)t.dim * m * es);
+  if (t.nslots) t.partials.ensure((size_t)t.nslots * m);
+}
+
+void s3ttmc_run(TensorState &t, const void *dU, uint32_t R, bool packed, void *dY, int precision,
+                cudaStream_t st) {
+  s3ttmc_reserve(t, R, packed, precision);
+  ItemSet all;
+  all.chunks = t.chunks.p;
+  all.nchunks = t.nchunks;
+  all.split = t.split.p;
+  all.nsplit = t.nsplit;
+  all.row0 = 0;
+  all.rows = t.dim;
+  s3ttmc_items(t, all, dU, R, packed, dY, precision, st);
+}
+
+// The compute and copy streams of the host-pointer call: created once per
+// device, one right after the other, and kept for the life of the process.
+static void host_streams(cudaStream_t &st, cudaStream_t &cp) {
+  static std::mutex mu;
+  static std::map<int, std::pair<cudaStream_t, cudaStream_t>> streams;
+  int dev = 0;
+  SPB_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(mu);
+  auto it = streams.find(dev);
+  if (it == streams.end()) {
+    cudaStream_t a, b;
+    SPB_CUDA(cudaStreamCreateWithFlags(&a, cudaStreamNonBlocking));
+    SPB_CUDA(cudaStreamCreateWithFlags(&b, cudaStreamNonBlocking));
+    it = streams.emplace(dev, std::make_pair(a, b)).first;
+  }
+  st = it->second.first;
+  cp = it->second.second;
+}
+
+// Number of row bands of the host-pointer call: one per 16 MiB of Y, at most
+// 16 (SPB_HOST_BANDS overrides; one band = no overlap).  Each band costs a
+// kernel tail; the last band's copy is not hidden.  On B200 over PCIe 5 the
+// order-4 R=16 call (Y = 653 MB FP64) took 26.4 ms with 1 band, 16.8 with 8,
+// 16.4 with 16 and 17.7 with 32 (compute alone 14.7 ms, copy alone 12 ms).
+static uint32_t host_band_count(size_t ybytes) {
+  if (const char *e = std::getenv("SPB_HOST_BANDS")) {
+    const long v = std::strtol(e, nullptr, 10);
+    if (v >= 1) return (uint32_t)std::min<long>(v, 64);
+  }
+  const size_t per = 16ull << 20;
+  return (uint32_t)std::max<size_t>(1, std::min<size_t>(16, (ybytes + per - 1) / per));
+}
+
+void s3ttmc_host(TensorState &t, const void *U, uint32_t R, bool packed, void *Y, int precision) {
+  s3ttmc_reserve(t, R, packed, precision);
+  const size_t es = precision == SYMPROP_FP64 ? 8 : 4;
+  uint64_t cols = packed ? symsize(R, t.order - 1) : 1;
+  if (!packed)
+    for (uint32_t j = 0; j + 1 < t.order; ++j) cols *= R;
+  const size_t ubytes = (size_t)t.dim * R * es, ybytes = (size_t)t.dim * cols * es;
+  t.io_U.ensure(ubytes);
+  t.io_Y.ensure(ybytes);
+  const RowBands &bd = row_bands(t, host_band_count(ybytes));
+
+  // SPB_TRACE_HOST=1 prints when each band's compute and copy ended
+  const bool trace = std::getenv("SPB_TRACE_HOST") != nullptr;
+  // compute on `st`, copy the finished bands back on `cp`; the guard waits
+  // for both streams before the events go, also when a launch throws
+  struct Events {
+    cudaStream_t st = nullptr, cp = nullptr;
+    std::vector<cudaEvent_t> done, copied;
+    ~Events() {
+      cudaStreamSynchronize(st);
+      cudaStreamSynchronize(cp);
+      for (cudaEvent_t e : done) cudaEventDestroy(e);
+      for (cudaEvent_t e : copied) cudaEventDestroy(e);
+    }
+  } ss;
+  host_streams(ss.st, ss.cp);
+  const uint32_t nev = bd.nb + (trace ? 1 : 0);
+  for (uint32_t k = 0; k < nev; ++k) {
+    cudaEvent_t e;
+    SPB_CUDA(cudaEventCreateWithFlags(&e, trace ? cudaEventDefault : cudaEventDisableTiming));
+    ss.done.push_back(e);
+    if (trace) {
+      SPB_CUDA(cudaEventCreate(&e));
+      ss.copied.push_back(e);
+    }
+  }
+  if (trace) SPB_CUDA(cudaEventRecord(ss.done[bd.nb], ss.st));
+  SPB_CUDA(cudaMemcpyAsync(t.io_U.p, U, ubytes, cudaMemcpyHostToDevice, ss.st));
+  for (uint32_t k = 0; k < bd.nb; ++k) {
+    ItemSet band;
+    band.chunks = bd.chunks.p + bd.chunk0[k];
+    band.nchunks = bd.chunk0[k + 1] - bd.chunk0[k];
+    band.split = bd.split.p + bd.split0[k];
+    band.nsplit = bd.split0[k + 1] - bd.split0[k];
+    band.row0 = bd.row0[k];
+    band.rows = bd.row0[k + 1] - bd.row0[k];
+    s3ttmc_items(t, band, t.io_U.p, R, packed, t.io_Y.p, precision, ss.st);
+    SPB_CUDA(cudaEventRecord(ss.done[k], ss.st));
+  }
+  // all compute is queued before the first copy, so a copy into pageable
+  // memory (which returns only when done) does not hold back the kernels
+  for (uint32_t k = 0; k < bd.nb; ++k) {
+    const size_t off = (size_t)bd.row0[k] * cols * es, len = (size_t)(bd.row0[k + 1] - bd.row0[k]) * cols * es;
+    SPB_CUDA(cudaStreamWaitEvent(ss.cp, ss.done[k], 0));
+    if (len) SPB_CUDA(cudaMemcpyAsync((char *)Y + off, t.io_Y.p + off, len, cudaMemcpyDeviceToHost, ss.cp));
+    if (trace) SPB_CUDA(cudaEventRecord(ss.copied[k], ss.cp));
+  }
+  SPB_CUDA(cudaStreamSynchronize(ss.cp));
+  SPB_CUDA(cudaStreamSynchronize(ss.st));
+  if (trace)
+    for (uint32_t k = 0; k < bd.nb; ++k) {
+      float a = 0.f, b = 0.f;
+      SPB_CUDA(cudaEventElapsedTime(&a, ss.done[bd.nb], ss.done[k]));
+      SPB_CUDA(cudaEventElapsedTime(&b, ss.done[bd.nb], ss.copied[k]));
+      std::fprintf(stderr, "[s3ttmc host] band %u/%u rows %u..%u items %u: computed %.3f ms, copied %.3f ms\n", k,
+                   bd.nb, bd.row0[k], bd.row0[k + 1], bd.chunk0[k + 1] - bd.chunk0[k], a, b);
+    }
+  SPB_CUDA(cudaGetLastError());
+}
+
+// combine the partial rows of the set's split rows; unpack its rows if
+// requested
+static void finish_rows(TensorState &t, const ItemSet &items, uint64_t m, void *Ypk, bool packed, void *dY,
+                        uint32_t R, uint32_t L, int precision, cudaStream_t st) {
+  if (items.nsplit) {
+    dim3 grid(items.nsplit, (unsigned)((m + 31) / 32));
     if (precision == SYMPROP_FP64)
-      combine_kernel<double><<<grid, 256, 0, st>>>(t.split.p, t.partials.p, (uint32_t)m, Ypk, m);
+      combine_kernel<double><<<grid, 256, 0, st>>>(items.split, t.partials.p, (uint32_t)m, Ypk, m);
     else
-      combine_kernel<float><<<grid, 256, 0, st>>>(t.split.p, t.partials.p, (uint32_t)m, Ypk, m);
+      combine_kernel<float><<<grid, 256, 0, st>>>(items.split, t.partials.p, (uint32_t)m, Ypk, m);
     SPB_LAUNCH_CHECK();
   }
-  if (!packed) unpack_rows(Ypk, t.dim, R, L, dY, precision, st);
+  if (!packed && items.rows) {
+    uint64_t full = 1;
+    for (uint32_t j = 0; j < L; ++j) full *= R;
+    const size_t es = precision == SYMPROP_FP64 ? 8 : 4;
+    unpack_rows((const char *)Ypk + (size_t)items.row0 * m * es, items.rows, R, L,
+                (char *)dY + (size_t)items.row0 * full * es, precision, st);
+  }
 }
 
 static std::atomic<int> g_schedule{kScheduleAuto};

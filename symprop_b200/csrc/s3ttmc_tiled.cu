@@ -470,11 +470,11 @@ static void launch_tiled_l(uint32_t L, int NT, const TiledParams &tp, uint32_t n
   }
 }
 
-void tiled_launch(const TiledPlan &pl, const TensorState &t, const void *dU, void *dYpacked,
+void tiled_launch(const TiledPlan &pl, const TensorState &t, const ItemSet &items, const void *dU, void *dYpacked,
                   int precision, cudaStream_t st) {
   const int pi = precision == SYMPROP_FP64 ? 0 : 1;
   TiledParams tp{};
-  tp.chunks = t.chunks.p;
+  tp.chunks = items.chunks;
   tp.own_S = t.own_S.p;
   tp.own_c = pi == 0 ? (const void *)t.own_c64.p : (const void *)t.own_c32.p;
   tp.sstride = t.sstride;
@@ -504,9 +504,9 @@ void tiled_launch(const TiledPlan &pl, const TensorState &t, const void *dU, voi
   tp.ksz4 = pl.ksz4;
   tp.BO = pl.BO[pi];
   tp.G = pl.G;
-  if (!t.nchunks) return;
-  if (pi == 0) launch_tiled_l<double>(pl.L, pl.NT, tp, t.nchunks, pl.smem[0], st);
-  else launch_tiled_l<float>(pl.L, pl.NT, tp, t.nchunks, pl.smem[1], st);
+  if (!items.nchunks) return;
+  if (pi == 0) launch_tiled_l<double>(pl.L, pl.NT, tp, items.nchunks, pl.smem[0], st);
+  else launch_tiled_l<float>(pl.L, pl.NT, tp, items.nchunks, pl.smem[1], st);
 }
 
 }  // namespace spb

@@ -13,7 +13,7 @@ struct TiledPlan;
 std::shared_ptr<TiledPlan> tiled_plan(uint32_t N, uint32_t R);
 bool tiled_supported(const TiledPlan &pl);
 // Writes the packed Y (lexicographic columns) or the partial rows of split rows.
-void tiled_launch(const TiledPlan &pl, const TensorState &t, const void *dU, void *dYpacked,
+void tiled_launch(const TiledPlan &pl, const TensorState &t, const ItemSet &items, const void *dU, void *dYpacked,
                   int precision, cudaStream_t st);
 
 }  // namespace spb

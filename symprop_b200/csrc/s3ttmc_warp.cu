@@ -806,13 +806,13 @@ static void launch_w_l(uint32_t L, uint32_t NTL, bool team, const WarpParams &wp
   }
 }
 
-void warp_launch(const WarpPlan &pl, const TensorState &t, const void *dU, void *dYpacked, int precision,
-                 cudaStream_t st) {
-  if (!t.nchunks) return;
+void warp_launch(const WarpPlan &pl, const TensorState &t, const ItemSet &items, const void *dU, void *dYpacked,
+                 int precision, cudaStream_t st) {
+  if (!items.nchunks) return;
   const int pi = precision == SYMPROP_FP64 ? 0 : 1;
   WarpParams wp{};
-  wp.chunks = t.chunks.p;
-  wp.nchunks = t.nchunks;
+  wp.chunks = items.chunks;
+  wp.nchunks = items.nchunks;
   wp.own_S = t.own_S.p;
   wp.own_c = pi == 0 ? (const void *)t.own_c64.p : (const void *)t.own_c32.p;
   wp.sstride = t.sstride;
@@ -842,8 +842,8 @@ void warp_launch(const WarpPlan &pl, const TensorState &t, const void *dU, void 
   wp.rowoff = pl.rowoff.p;
   wp.ntiles = pl.ntiles;
   wp.wsz = pl.wsz;
-  if (pi == 0) launch_w_l<double>(pl.L, pl.NTL, pl.team, wp, t.nchunks, pl.smem[0], st);
-  else launch_w_l<float>(pl.L, pl.NTL, pl.team, wp, t.nchunks, pl.smem[1], st);
+  if (pi == 0) launch_w_l<double>(pl.L, pl.NTL, pl.team, wp, items.nchunks, pl.smem[0], st);
+  else launch_w_l<float>(pl.L, pl.NTL, pl.team, wp, items.nchunks, pl.smem[1], st);
 }
 
 }  // namespace spb

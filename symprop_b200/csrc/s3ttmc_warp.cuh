@@ -10,7 +10,7 @@ namespace spb {
 struct WarpPlan;
 std::shared_ptr<WarpPlan> warp_plan(uint32_t N, uint32_t R);
 bool warp_supported(const WarpPlan &pl);
-void warp_launch(const WarpPlan &pl, const TensorState &t, const void *dU, void *dYpacked,
+void warp_launch(const WarpPlan &pl, const TensorState &t, const ItemSet &items, const void *dU, void *dYpacked,
                  int precision, cudaStream_t st);
 
 }  // namespace spb

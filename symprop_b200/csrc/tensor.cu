@@ -128,6 +128,31 @@ inline unsigned grid_for(uint64_t n, unsigned block) {
 
 }  // namespace
 
+// The work items in row order: one chunk per row, rows with more than
+// t.chunk_owners owners cut into consecutive slices, each slice with its own
+// partial-sum slot.  Returns the number of slots.
+static uint32_t row_order_items(const TensorState &t, std::vector<Chunk> &ch, std::vector<SplitRow> &sp) {
+  const uint64_t co = t.chunk_owners;
+  ch.clear();
+  sp.clear();
+  ch.reserve((size_t)t.dim + t.nown / co + 1);
+  uint32_t slot = 0;
+  for (uint32_t i = 0; i < t.dim; ++i) {
+    uint64_t b = t.h_row_ptr[i], e = t.h_row_ptr[(size_t)i + 1];
+    uint64_t c = e - b;
+    if (c <= co) {
+      ch.push_back(Chunk{i, kDirect, b, e});
+    } else {
+      uint32_t s0 = slot;
+      for (uint64_t x = b; x < e; x += co) ch.push_back(Chunk{i, slot++, x, std::min(e, x + co)});
+      sp.push_back(SplitRow{i, s0, slot, 0});
+    }
+  }
+  return slot;
+}
+
+static bool heavier(const Chunk &a, const Chunk &b) { return (a.oe - a.ob) > (b.oe - b.ob); }
+
 void tensor_build(TensorState &t, const uint32_t *h_inds, const double *h_vals, bool on_device) {
   const uint32_t N = t.order;
   const uint64_t nnz = t.nnz;
@@ -236,22 +261,8 @@ void tensor_build(TensorState &t, const uint32_t *h_inds, const double *h_vals, 
   t.chunk_owners = (uint32_t)co;
   std::vector<Chunk> ch;
   std::vector<SplitRow> sp;
-  ch.reserve((size_t)t.dim + t.nown / co + 1);
-  uint32_t slot = 0;
-  for (uint32_t i = 0; i < t.dim; ++i) {
-    uint64_t b = t.h_row_ptr[i], e = t.h_row_ptr[(size_t)i + 1];
-    uint64_t c = e - b;
-    if (c <= co) {
-      ch.push_back(Chunk{i, kDirect, b, e});
-    } else {
-      uint32_t s0 = slot;
-      for (uint64_t x = b; x < e; x += co) ch.push_back(Chunk{i, slot++, x, std::min(e, x + co)});
-      sp.push_back(SplitRow{i, s0, slot, 0});
-    }
-  }
-  std::stable_sort(ch.begin(), ch.end(), [](const Chunk &a, const Chunk &b) {
-    return (a.oe - a.ob) > (b.oe - b.ob);
-  });
+  const uint32_t slot = row_order_items(t, ch, sp);
+  std::stable_sort(ch.begin(), ch.end(), heavier);
   t.nchunks = (uint32_t)ch.size();
   t.nheavy = 0;
   while (t.nheavy < t.nchunks && ch[t.nheavy].oe - ch[t.nheavy].ob > kLightOwners) ++t.nheavy;
@@ -263,7 +274,41 @@ void tensor_build(TensorState &t, const uint32_t *h_inds, const double *h_vals, 
   t.split.alloc(sp.size());
   if (!sp.empty())
     SPB_CUDA(cudaMemcpy(t.split.p, sp.data(), sp.size() * sizeof(SplitRow), cudaMemcpyHostToDevice));
+  t.bands.reset();
   SPB_CUDA(cudaDeviceSynchronize());
+}
+
+const RowBands &row_bands(TensorState &t, uint32_t nb) {
+  nb = std::max<uint32_t>(1, std::min<uint32_t>(nb, std::max<uint32_t>(t.dim, 1)));
+  if (t.bands && t.bands->nb == nb) return *t.bands;
+  auto b = std::make_unique<RowBands>();
+  b->nb = nb;
+  std::vector<Chunk> ch;
+  std::vector<SplitRow> sp;
+  row_order_items(t, ch, sp);
+  b->row0.resize(nb + 1);
+  b->chunk0.resize(nb + 1);
+  b->split0.resize(nb + 1);
+  for (uint32_t k = 0; k <= nb; ++k) {
+    const uint32_t r = (uint32_t)((uint64_t)t.dim * k / nb);
+    b->row0[k] = r;
+    b->chunk0[k] = (uint32_t)(std::lower_bound(ch.begin(), ch.end(), r,
+                                               [](const Chunk &c, uint32_t v) { return c.row < v; }) -
+                              ch.begin());
+    b->split0[k] = (uint32_t)(std::lower_bound(sp.begin(), sp.end(), r,
+                                               [](const SplitRow &c, uint32_t v) { return c.row < v; }) -
+                              sp.begin());
+  }
+  for (uint32_t k = 0; k < nb; ++k)
+    std::stable_sort(ch.begin() + b->chunk0[k], ch.begin() + b->chunk0[k + 1], heavier);
+  b->chunks.alloc(ch.size());
+  if (!ch.empty())
+    SPB_CUDA(cudaMemcpy(b->chunks.p, ch.data(), ch.size() * sizeof(Chunk), cudaMemcpyHostToDevice));
+  b->split.alloc(sp.size());
+  if (!sp.empty())
+    SPB_CUDA(cudaMemcpy(b->split.p, sp.data(), sp.size() * sizeof(SplitRow), cudaMemcpyHostToDevice));
+  t.bands = std::move(b);
+  return *t.bands;
 }
 
 }  // namespace spb

@@ -46,6 +46,29 @@ struct SplitRow {
   uint32_t pad;
 };
 
+// The work items regrouped into nb bands of consecutive rows (band k holds
+// rows [row0[k], row0[k+1]), its chunks [chunk0[k], chunk0[k+1]) heaviest
+// first, and its split rows [split0[k], split0[k+1])).  The host-pointer
+// S3TTMc runs the bands one after another so that the rows of one band are
+// copied to the host while the next band is computed.  Slots are the ones of
+// TensorState::split, so a band writes the same partial sums.
+struct RowBands {
+  uint32_t nb = 0;
+  std::vector<uint32_t> row0, chunk0, split0;
+  DBuf<Chunk> chunks;
+  DBuf<SplitRow> split;
+};
+
+// The work items of one S3TTMc pass: all of them, or one row band.  After the
+// pass Y rows [row0, row0 + rows) are complete.
+struct ItemSet {
+  const Chunk *chunks = nullptr;
+  uint32_t nchunks = 0;
+  const SplitRow *split = nullptr;
+  uint32_t nsplit = 0;
+  uint32_t row0 = 0, rows = 0;
+};
+
 // Reference CompressedDTree arrays, built on demand (tree.cu).
 struct TreeLevels {
   uint32_t depth = 0;
@@ -104,11 +127,15 @@ struct TensorState {
   std::map<uint32_t, std::shared_ptr<TiledPlan>> tiled;      // by R
   std::map<uint32_t, std::shared_ptr<WarpPlan>> warp;        // by R
   std::unique_ptr<TreeLevels> tree;
+  std::unique_ptr<RowBands> bands;
 };
 
 // s3ttmc.cu
 void s3ttmc_run(TensorState &t, const void *dU, uint32_t R, bool packed, void *dY,
                 int precision, cudaStream_t stream);
+// host U in, host Y out; the result rows are copied back band by band while
+// the later bands are computed
+void s3ttmc_host(TensorState &t, const void *U, uint32_t R, bool packed, void *Y, int precision);
 uint32_t s3ttmc_launch_count(const TensorState &t, uint32_t R, bool packed);
 void unpack_rows(const void *dpacked, uint64_t rows, uint32_t dim, uint32_t order,
                  void *dfull, int precision, cudaStream_t stream);
@@ -117,6 +144,8 @@ void tree_build(TensorState &t);
 // tensor.cu
 // inds/vals in host memory, or in device memory when on_device is set
 void tensor_build(TensorState &t, const uint32_t *inds, const double *vals, bool on_device = false);
+// the work items in nb row bands (built on first use, kept for the next call)
+const RowBands &row_bands(TensorState &t, uint32_t nb);
 
 }  // namespace spb
 

@@ -137,3 +137,35 @@ def test_device_pointer_entry_point_with_torch_stream(gpu):
     s.synchronize()
     assert rel(dY.cpu().numpy(), orc.s3ttmc(order, n, t, v, U, R, True)) < FP64_TOL
     assert X.s3ttmc_launches(R, True) >= 1
+
+
+@pytest.mark.parametrize("bands", [1, 2, 5, 64])
+def test_host_call_row_bands_match_device_call(gpu, schedule, bands, monkeypatch):
+    """The host-pointer call runs the work items in row bands and copies each
+    band back while the next is computed; every band count gives the device
+    call's result bit for bit, packed and full, FP64 and FP32, with split hub
+    rows, empty rows and more bands than rows."""
+    import torch
+    monkeypatch.setenv("SPB_HOST_BANDS", str(bands))
+    rng = np.random.default_rng(bands)
+    cases = []
+    for order, n, nnz, R in [(4, 300, 6000, 6), (5, 90, 3000, 4), (3, 40, 500, 7), (2, 12, 20, 3), (4, 3, 6, 2)]:
+        t = synth.zipf_tuples(order, n, nnz, 1.2, 11 + order)
+        if order == 4 and n == 300:  # hub row: every tuple holds id 1
+            t = np.unique(np.sort(np.concatenate([np.ones((nnz, 1), np.uint32), t[:, 1:]], axis=1), axis=1),
+                          axis=0)
+        cases.append((order, n, t, synth.uniform_values(t.shape[0], 3), R))
+    for order, n, t, v, R in cases:
+        X = gpu.SpSymtensor(n, order, t, v)
+        U = rng.standard_normal((n, R))
+        for prec, dt in ((gpu.FP64, torch.float64), (gpu.FP32, torch.float32)):
+            Uc = U.astype(np.float64 if prec == gpu.FP64 else np.float32)
+            for packed in (True, False):
+                Yh = run_or_skip(gpu, schedule, lambda: X.S3TTMc(Uc, R, packed, precision=prec))
+                dU = torch.from_numpy(Uc).cuda()
+                dY = torch.full(Yh.shape, float("nan"), dtype=dt, device="cuda")
+                X.s3ttmc_device(dU.data_ptr(), R, dY.data_ptr(), packed, prec)
+                torch.cuda.synchronize()
+                np.testing.assert_array_equal(Yh, dY.cpu().numpy(), err_msg=f"{order} {n} {prec} {packed}")
+                if prec == gpu.FP64 and packed:
+                    assert rel(Yh, orc.s3ttmc(order, n, t, v, U, R, True)) < FP64_TOL
