@@ -174,6 +174,45 @@ int symprop_gram_device(const void *dY, uint64_t n, uint32_t m, const void *dsca
 int symprop_gram_device_noalloc(const float *dY, uint64_t n, uint32_t m, const float *dscale,
                                 double *dG, void *stream);
 
+/* ------------------------------------------- matrix:: operations (host) */
+/* FP64 row-major matrices in host memory, computed on the current device:
+ * the operations of the reference's symprop::matrix namespace
+ * (include/detail/dense/matrixops.hpp:12-45, src/dense/matrixops.cpp).
+ * Each copies its operands to the device and its result back. */
+
+/* C (acol x bcol) = A^T B; A is arow x acol, B is arow x bcol
+ * (matrix::gemmtn, src/dense/matrixops.cpp:45-56). */
+int symprop_gemmtn(double *C, const double *A, const double *B, uint64_t arow, uint64_t acol,
+                   uint64_t bcol);
+
+/* C (I1 x I2) = A diag(row_coeff) B^T; A is I1 x ncoeff, B is I2 x ncoeff
+ * (matrix::symgemm, :102-124). */
+int symprop_symgemm(double *C, const double *A, const double *B, const double *row_coeff,
+                    uint64_t ncoeff, uint64_t I1, uint64_t I2);
+
+/* Upper triangle (j >= i) of C (I1 x I1) = A diag(row_coeff) A^T; A is
+ * I1 x ncoeff; the strict lower triangle of C is left as it was, as
+ * cblas_dsyrk(CblasUpper) leaves it (matrix::symsyrk, :126-146). */
+int symprop_symsyrk(double *C, const double *A, const double *row_coeff, uint64_t ncoeff,
+                    uint64_t I1);
+
+/* A (nr x nc, nr >= nc) replaced in place by the explicit Q of its
+ * Householder QR, with LAPACK's dgeqrf/dorgqr reflector convention
+ * (matrix::qr, :58-75). */
+int symprop_qr(double *A, uint64_t nr, uint64_t nc);
+
+/* U (dim x rank) = eigenvectors of the rank largest eigenvalues of the
+ * symmetric dim x dim matrix A, in ascending eigenvalue order as dsyevd
+ * returns them (matrix::syevd, :77-100).  A is not modified (the reference
+ * leaves dsyevd's eigenvectors in it).  rank <= 48 when dim > 96. */
+int symprop_syevd(const double *A, double *U, uint64_t dim, uint64_t rank);
+
+/* U (nr x rank) = the rank leading left singular vectors of A (nr x nc),
+ * in descending singular-value order, from the eigenvectors of the smaller
+ * Gram matrix (matrix::leftsvd, :18-43).  A is not modified (the reference
+ * leaves dgesvd's left vectors in it).  rank <= min(nr, nc). */
+int symprop_leftsvd(const double *A, double *U, uint64_t nr, uint64_t nc, uint64_t rank);
+
 /* ------------------------------------------------------------- Tucker */
 typedef struct {
   uint32_t rank;      /* Config::rank     (include/detail/tucker.hpp:15) */

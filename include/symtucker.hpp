@@ -16,8 +16,10 @@
 #define SYMPROP_SYMTUCKER_HPP
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdint>
+#include <cstdio>
 #include <fstream>
 #include <iomanip>
 #include <iostream>
@@ -153,6 +155,83 @@ class SymTuckerDecomp {  // include/detail/tucker.hpp:25-45
   double _time_ms = 0;
 };
 
+// --------------------------------------------------------------- matrix
+// The reference's dense operations (include/detail/dense/matrixops.hpp:12-45,
+// src/dense/matrixops.cpp:18-146) with the same signatures, computed on the
+// GPU (symprop_gemmtn, ...).  As in the reference, a solver that does not
+// converge prints its message and returns; the output then holds the last
+// iterate.  Two differences: syevd and leftsvd leave A unchanged (LAPACK
+// overwrites it with eigen- / singular vectors), and singular or
+// eigenvector signs are the device solver's, not LAPACK's.
+namespace matrix {
+
+namespace detail {
+struct Timed {  // records the call in FunctionTimer as START_FUNCTION_TIMER does
+  const char *name;
+  std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
+  ~Timed() {
+    FunctionTimer::add(
+        name, std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count());
+  }
+};
+inline void need(bool ok, const char *what) {
+  if (!ok) throw std::runtime_error(std::string("matrix::") + what + ": operand has the wrong size");
+}
+inline void solved(int st, const char *message) {
+  if (st == SYMPROP_ERR_NOCONV) std::printf("%s\n", message);
+  else check_status(st);
+}
+}  // namespace detail
+
+// U (nr x rank) = leading left singular vectors of A (nr x nc)
+inline void leftsvd(std::vector<real_t> &A, std::vector<real_t> &U, size_t nr, size_t nc, size_t rank) {
+  detail::Timed t{"leftsvd"};
+  detail::need(A.size() >= nr * nc && U.size() >= nr * rank, "leftsvd");
+  detail::solved(symprop_leftsvd(A.data(), U.data(), nr, nc, rank), "SVD failed to converge.");
+}
+
+// C (acol x bcol) = A^T B
+inline void gemmtn(std::vector<real_t> &C, const std::vector<real_t> &A, const std::vector<real_t> &B,
+                   size_t arow, size_t acol, size_t bcol) {
+  detail::Timed t{"gemmtn"};
+  detail::need(A.size() >= arow * acol && B.size() >= arow * bcol && C.size() >= acol * bcol, "gemmtn");
+  check_status(symprop_gemmtn(C.data(), A.data(), B.data(), arow, acol, bcol));
+}
+
+// A (nr x nc) = Q of its QR decomposition
+inline void qr(std::vector<real_t> &A, size_t nr, size_t nc) {
+  detail::Timed t{"qr"};
+  detail::need(A.size() >= nr * nc, "qr");
+  check_status(symprop_qr(A.data(), nr, nc));
+}
+
+// U (dim x rank) = eigenvectors of the rank largest eigenvalues, ascending
+inline void syevd(std::vector<real_t> &A, std::vector<real_t> &U, size_t dim, size_t rank) {
+  detail::Timed t{"syevd"};
+  detail::need(A.size() >= dim * dim && U.size() >= dim * rank, "syevd");
+  detail::solved(symprop_syevd(A.data(), U.data(), dim, rank), "Eigendecomposition failed to converge.");
+}
+
+// C (I1 x I2) = A diag(row_coeff) B^T
+inline void symgemm(std::vector<real_t> &C, const std::vector<real_t> &A, const std::vector<real_t> &B,
+                    const std::vector<real_t> &row_coeff, size_t I1, size_t I2) {
+  detail::Timed t{"symgemm"};
+  const size_t m = row_coeff.size();
+  detail::need(A.size() == I1 * m && B.size() == I2 * m && C.size() >= I1 * I2, "symgemm");
+  check_status(symprop_symgemm(C.data(), A.data(), B.data(), row_coeff.data(), m, I1, I2));
+}
+
+// upper triangle of C (I1 x I1) = A diag(row_coeff) A^T
+inline void symsyrk(std::vector<real_t> &C, const std::vector<real_t> &A, const std::vector<real_t> &row_coeff,
+                    size_t I1) {
+  detail::Timed t{"symsyrk"};
+  const size_t m = row_coeff.size();
+  detail::need(A.size() == I1 * m && C.size() == I1 * I1, "symsyrk");
+  check_status(symprop_symsyrk(C.data(), A.data(), row_coeff.data(), m, I1));
+}
+
+}  // namespace matrix
+
 // ------------------------------------------------------------ SpSymtensor
 class SpSymtensor {  // include/detail/sparse/spsymtensor.hpp:24-65
  public:
@@ -193,6 +272,7 @@ class SpSymtensor {  // include/detail/sparse/spsymtensor.hpp:24-65
                                   : (size_t)std::llround(std::pow((double)R, (double)_order - 1));
     if (res.size() != (size_t)_dim * cols) throw std::runtime_error("S3TTMc: res has wrong size");
     if (U.size() != (size_t)_dim * R) throw std::runtime_error("S3TTMc: U has wrong size");
+    matrix::detail::Timed t{"S3TTMc"};
     check_status(
         symprop_s3ttmc(_t.get(), U.data(), R, partial_sym_res ? 1 : 0, res.data(), SYMPROP_FP64));
   }

@@ -19,6 +19,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libsymprop_b200.so")
 CLI_PATH = os.path.join(HERE, "symtucker")
+TTMC_PATH = os.path.join(HERE, "symtens_ttmc")
+TTMCTC_PATH = os.path.join(HERE, "s3ttmctc")
 
 SYMPROP_OK = 0
 ERR_INVALID, ERR_ORDER, ERR_OOM, ERR_CUDA, ERR_NOCONV, ERR_TIMEOUT, ERR_SIZE, ERR_NODEVICE = range(1, 9)
@@ -52,7 +54,7 @@ _lib = None
 
 
 def build(force: bool = False) -> None:
-    """Compile libsymprop_b200.so and the symtucker CLI for sm_100a (make)."""
+    """Compile libsymprop_b200.so, the symtucker CLI and the symtens_ttmc / s3ttmctc drivers (make; sm_100a)."""
     cmd = ["make", "-C", HERE, "-j8"]
     if force:
         subprocess.run(["make", "-C", HERE, "clean"], check=True)
@@ -97,6 +99,12 @@ def lib():
         "symprop_gram_device_noalloc": (_I, [_P, _U64, _U32, _P, _P, _P]),
         "symprop_tensor_load_tns": (_I, [ctypes.c_char_p, ctypes.POINTER(_P)]),
         "symprop_tensor_copy_nonzeros": (_I, [_P, _P, _P]),
+        "symprop_gemmtn": (_I, [_P, _P, _P, _U64, _U64, _U64]),
+        "symprop_symgemm": (_I, [_P, _P, _P, _P, _U64, _U64, _U64]),
+        "symprop_symsyrk": (_I, [_P, _P, _P, _U64, _U64]),
+        "symprop_qr": (_I, [_P, _U64, _U64]),
+        "symprop_syevd": (_I, [_P, _P, _U64, _U64]),
+        "symprop_leftsvd": (_I, [_P, _P, _U64, _U64, _U64]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -116,6 +124,7 @@ def exported_symbols() -> list[str]:
         "symprop_symtens_size", "symprop_symtens_coeff", "symprop_unpack_rows_device", "symprop_tucker",
         "symprop_write_decomp", "symprop_gram_device", "symprop_s3ttmc_schedule",
         "symprop_tensor_load_tns", "symprop_tensor_copy_nonzeros",
+        "symprop_gemmtn", "symprop_symgemm", "symprop_symsyrk", "symprop_qr", "symprop_syevd", "symprop_leftsvd",
     ]
 
 
@@ -140,6 +149,60 @@ def gram_device(dY_ptr: int, n: int, m: int, dscale_ptr: int, dG_ptr: int, preci
     """G = (Y diag(scale))^T (Y diag(scale)) on the device (FP64 CUDA cores or
     FP32 input on tcgen05 tensor cores with split-BF16 operands)."""
     _check(lib().symprop_gram_device(_P(dY_ptr), n, m, _P(dscale_ptr), _P(dG_ptr), precision, _P(stream)))
+
+
+class matrix:
+    """The reference's symprop::matrix operations (src/dense/matrixops.cpp:18-146)
+    on FP64 row-major arrays, computed on the GPU.  Functions return new arrays
+    instead of writing into the caller's; symsyrk fills the upper triangle of
+    the C it is given (the rest is kept) as cblas_dsyrk does."""
+
+    @staticmethod
+    def _f64(a, shape):
+        return np.ascontiguousarray(a, dtype=np.float64).reshape(shape)
+
+    @staticmethod
+    def gemmtn(A, B, arow: int, acol: int, bcol: int) -> np.ndarray:
+        A, B = matrix._f64(A, (arow, acol)), matrix._f64(B, (arow, bcol))
+        C = np.zeros((acol, bcol))
+        _check(lib().symprop_gemmtn(_ptr(C), _ptr(A), _ptr(B), arow, acol, bcol))
+        return C
+
+    @staticmethod
+    def symgemm(A, B, row_coeff, I1: int, I2: int) -> np.ndarray:
+        c = np.ascontiguousarray(row_coeff, dtype=np.float64).reshape(-1)
+        A, B = matrix._f64(A, (I1, c.size)), matrix._f64(B, (I2, c.size))
+        C = np.zeros((I1, I2))
+        _check(lib().symprop_symgemm(_ptr(C), _ptr(A), _ptr(B), _ptr(c), c.size, I1, I2))
+        return C
+
+    @staticmethod
+    def symsyrk(C, A, row_coeff, I1: int) -> np.ndarray:
+        c = np.ascontiguousarray(row_coeff, dtype=np.float64).reshape(-1)
+        A = matrix._f64(A, (I1, c.size))
+        C = matrix._f64(C, (I1, I1)).copy()
+        _check(lib().symprop_symsyrk(_ptr(C), _ptr(A), _ptr(c), c.size, I1))
+        return C
+
+    @staticmethod
+    def qr(A, nr: int, nc: int) -> np.ndarray:
+        A = matrix._f64(A, (nr, nc)).copy()
+        _check(lib().symprop_qr(_ptr(A), nr, nc))
+        return A
+
+    @staticmethod
+    def syevd(A, dim: int, rank: int) -> np.ndarray:
+        A = matrix._f64(A, (dim, dim))
+        U = np.zeros((dim, rank))
+        _check(lib().symprop_syevd(_ptr(A), _ptr(U), dim, rank))
+        return U
+
+    @staticmethod
+    def leftsvd(A, nr: int, nc: int, rank: int) -> np.ndarray:
+        A = matrix._f64(A, (nr, nc))
+        U = np.zeros((nr, rank))
+        _check(lib().symprop_leftsvd(_ptr(A), _ptr(U), nr, nc, rank))
+        return U
 
 
 def symtens_size(dim: int, order: int) -> int:

@@ -1,7 +1,8 @@
 """Regenerates the golden fixtures in tests/golden/ by running the reference
 SymProp itself (its own sources compiled into oracle/_ref by oracle/Makefile).
 
-    make -C oracle ref && python tests/golden/make_golden.py
+    make -C oracle ref && python tests/golden/make_golden.py          # all fixtures
+    make -C oracle ref && python tests/golden/make_golden.py ttmc     # ttmc.npz only
 
 Fixtures (all small):
   trees.npz     CompressedDTree arrays (level_idx, level_ptr, dep_list,
@@ -13,6 +14,8 @@ Fixtures (all small):
                 AltHOOI (symtucker CLI) on seeded tensors, and on the shipped
                 examples/contact-5.tns when present (numbers only; the input
                 file itself is not copied)
+  ttmc.npz      the reference's examples/symtens_ttmc driver run on seeded
+                .tns files: the input text, the driver's ttmc.out bytes
 """
 import json
 import os
@@ -30,6 +33,7 @@ from symprop_b200 import synth  # noqa: E402
 OUT = os.path.dirname(os.path.abspath(__file__))
 PROBE = os.path.join(ROOT, "oracle", "_ref", "ref_probe")
 CLI = os.path.join(ROOT, "oracle", "_ref", "symtucker")
+TTMC = os.path.join(ROOT, "oracle", "_ref", "symtens_ttmc")
 CONTACT5 = "/root/reference/examples/contact-5.tns"
 
 TREE_CASES = [  # order, n, nnz, seed
@@ -39,6 +43,10 @@ TREE_CASES = [  # order, n, nnz, seed
 Y_CASES = [  # order, n, nnz, seed, R
     (3, 25, 120, 21, 3), (3, 30, 200, 22, 7), (4, 30, 300, 23, 4), (4, 50, 600, 24, 6),
     (5, 20, 250, 25, 3), (5, 40, 500, 26, 5), (6, 15, 150, 27, 3), (4, 8, 60, 28, 16),
+]
+TTMC_CASES = [  # order, n, nnz, seed, R
+    (3, 40, 300, 41, 4), (4, 60, 800, 42, 5), (5, 30, 400, 43, 3), (2, 10, 20, 44, 3), (6, 12, 100, 45, 2),
+    (4, 120, 2000, 46, 8),
 ]
 TUCKER_CASES = [  # name, order, n, nnz, seed, R, iters, delta, s
     ("o3_n60", 3, 60, 800, 31, 4, 15, 0.5, 1.2),
@@ -89,8 +97,31 @@ def parse_iters(text):
     return runs
 
 
+def make_ttmc(tmp):
+    out = {}
+    for ci, (order, n, nnz, seed, R) in enumerate(TTMC_CASES):
+        t = synth.zipf_tuples(order, n, nnz, 1.2, seed)
+        v = synth.uniform_values(nnz, seed)
+        d = os.path.join(tmp, f"ttmc{ci}")
+        os.makedirs(d)
+        tns = os.path.join(d, "x.tns")
+        synth.write_tns(tns, order, n, t, v)
+        subprocess.run([TTMC, tns, str(R)], check=True, capture_output=True, cwd=d,
+                       env=dict(os.environ, OMP_NUM_THREADS="8"))
+        out[f"c{ci}_meta"] = np.array([order, n, nnz, seed, R], np.int64)
+        out[f"c{ci}_tns"] = np.frombuffer(open(tns, "rb").read(), np.uint8)
+        out[f"c{ci}_out"] = np.frombuffer(open(os.path.join(d, "ttmc.out"), "rb").read(), np.uint8)
+    np.savez_compressed(os.path.join(OUT, "ttmc.npz"), **out)
+
+
 def main():
     tmp = tempfile.mkdtemp()
+    want = set(sys.argv[1:]) or {"trees", "s3ttmc", "tucker", "ttmc"}
+    if "ttmc" in want:
+        make_ttmc(tmp)
+    if not want & {"trees", "s3ttmc", "tucker"}:
+        print("wrote", os.listdir(OUT))
+        return
     trees = {}
     for ci, (order, n, nnz, seed) in enumerate(TREE_CASES):
         t = synth.zipf_tuples(order, n, nnz, 1.2, seed)

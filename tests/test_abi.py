@@ -54,3 +54,18 @@ def test_cli_help_and_unknown_flag():
     assert r.returncode == 1 and "-f <input_file>" in r.stdout
     r = subprocess.run([cli, "-zz"], capture_output=True, text=True)
     assert r.returncode == 1 and "Option -zz is not defined" in r.stdout
+
+
+def test_symtens_ttmc_usage_and_open_failure(tmp_path):
+    """examples/symtens_ttmc.cpp:12-27: fewer than two arguments print the
+    usage line, an unreadable file the open error; both exit 1 before any
+    device work."""
+    exe = sp.TTMC_PATH
+    r = subprocess.run([exe], capture_output=True, text=True)
+    assert r.returncode == 1 and r.stderr == f"Usage: {exe} <input_file> <R>\n"
+    r = subprocess.run([exe, "only-one"], capture_output=True, text=True)
+    assert r.returncode == 1 and r.stderr.startswith("Usage: ")
+    missing = str(tmp_path / "none.tns")
+    r = subprocess.run([exe, missing, "4"], capture_output=True, text=True, cwd=tmp_path)
+    assert r.returncode == 1 and r.stderr == f"Error opening file: {missing}\n"
+    assert not (tmp_path / "ttmc.out").exists()
