@@ -112,3 +112,31 @@ def test_cli_matches_reference_lines(gpu, tmp_path):
     assert all(len(l.rstrip(",").split(",")) == R ** (N - 1) for l in blk[1:1 + R])
     assert blk[1 + R] == "Factor U:"
     assert all(len(l.rstrip(",").split(",")) == R for l in blk[2 + R:])
+
+
+def test_cli_reads_malformed_text_as_the_reference_loader(gpu, tmp_path):
+    """The CLI parses .tns on the device; text the device parser rejects goes
+    through SymtensLoader (src/utils/loader.cpp:15-33), which keeps the
+    records read before the stream fails.  A value token `2.5x` is read as
+    2.5, then the stream fails on `x`: the file then gives the same HOOI as
+    the clean file cut after that record."""
+    case = golden()["o3_n60"]
+    N, n = case["order"], case["n"]
+    t = synth.zipf_tuples(N, n, case["nnz"], case["zipf"], case["seed"])
+    v = np.ones(case["nnz"])
+    cut = case["nnz"] // 2
+    v[cut - 1] = 2.5
+    clean, bad = tmp_path / "clean.tns", tmp_path / "bad.tns"
+    synth.write_tns(str(clean), N, n, t[:cut], v[:cut])
+    synth.write_tns(str(bad), N, n, t, v)
+    lines = bad.read_text().splitlines()
+    lines[cut] = lines[cut].rsplit(" ", 1)[0] + " 2.5x"
+    bad.write_text("\n".join(lines) + "\n")
+
+    def errors(path):
+        r = subprocess.run([gpu.CLI_PATH, "-f", str(path), "-r", "4", "-i", "4", "-d", "0.5", "-s", "0", "-a", "0"],
+                           capture_output=True, text=True, timeout=300)
+        assert r.returncode == 0, r.stderr
+        return [l.split(" error ")[1] for l in r.stdout.splitlines() if l.startswith("Iteration: ")]
+
+    assert errors(bad) == errors(clean)
