@@ -571,18 +571,20 @@ static void host_streams(cudaStream_t &st, cudaStream_t &cp) {
   cp = it->second.second;
 }
 
-// Number of row bands of the host-pointer call: one per 16 MiB of Y, at most
-// 16 (SPB_HOST_BANDS overrides; one band = no overlap).  Each band costs a
-// kernel tail; the last band's copy is not hidden.  On B200 over PCIe 5 the
-// order-4 R=16 call (Y = 653 MB FP64) took 26.4 ms with 1 band, 16.8 with 8,
-// 16.4 with 16 and 17.7 with 32 (compute alone 14.7 ms, copy alone 12 ms).
+// Number of row bands of the host-pointer call: one per 40 MiB of Y (about
+// 0.75 ms of PCIe copy), at most 64 (SPB_HOST_BANDS overrides; one band = no
+// overlap).  Each band costs a kernel tail; the last band's copy is not
+// hidden.  On B200 over PCIe 5 the order-4 R=16 call (Y = 653 MB FP64) took
+// 26.4 ms with 1 band, 16.8 with 8, 16.4 with 16 and 17.7 with 32 (compute
+// alone 14.7 ms, copy alone 12 ms); an order-5 call with Y = 1.55 GB was
+// flat (116.2-116.5 ms) from 16 to 48 bands.
 static uint32_t host_band_count(size_t ybytes) {
   if (const char *e = std::getenv("SPB_HOST_BANDS")) {
     const long v = std::strtol(e, nullptr, 10);
     if (v >= 1) return (uint32_t)std::min<long>(v, 64);
   }
-  const size_t per = 16ull << 20;
-  return (uint32_t)std::max<size_t>(1, std::min<size_t>(16, (ybytes + per - 1) / per));
+  const size_t per = 40ull << 20;
+  return (uint32_t)std::max<size_t>(1, std::min<size_t>(64, (ybytes + per - 1) / per));
 }
 
 void s3ttmc_host(TensorState &t, const void *U, uint32_t R, bool packed, void *Y, int precision) {
