@@ -5,6 +5,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <cstdarg>
 #include <cstdint>
@@ -40,6 +41,9 @@ void set_last_error(const std::string &msg);
 
 inline void cuda_check(cudaError_t e, const char *what, const char *file, int line) {
   if (e != cudaSuccess) {
+    // reset the runtime's last-error slot: a refused allocation (or another
+    // non-sticky error) would otherwise resurface at the next launch check
+    cudaGetLastError();
     int code = (e == cudaErrorMemoryAllocation) ? SYMPROP_ERR_OOM
                : (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver)
                    ? SYMPROP_ERR_NODEVICE
@@ -66,6 +70,17 @@ template <class F> int guard(F &&body) {
     return SYMPROP_ERR_INVALID;
   }
 }
+
+// ------------------------------------------------------------ NVTX ranges
+// Named host phases for nsys / ncu --nvtx (the GPU counterpart of the
+// reference's FunctionTimer scopes, src/utils/function_timer.cpp); the calls
+// do nothing unless a profiling tool is attached.
+struct NvtxRange {
+  explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange &) = delete;
+  NvtxRange &operator=(const NvtxRange &) = delete;
+};
 
 // ---------------------------------------------------------- device buffer
 

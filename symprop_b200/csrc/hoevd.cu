@@ -99,6 +99,7 @@ __global__ void scatter_kernel(const uint64_t *row_ptr, uint32_t dim, const uint
 // Top-r eigenvectors of A = X_(1) X_(1)^T without forming A (see above).
 // U: n x r device, row-major.  Returns the eigensolver status.
 int hoevd_matrix_free(TensorState &t, cudaStream_t st, int r, double *U) {
+  NvtxRange nv("hoevd (matrix-free)");
   tree_build(t);
   const TreeLevels &tr = *t.tree;
   const uint32_t lv = tr.depth - 1;

@@ -541,6 +541,7 @@ static void s3ttmc_reserve(TensorState &t, uint32_t R, bool packed, int precisio
 
 void s3ttmc_run(TensorState &t, const void *dU, uint32_t R, bool packed, void *dY, int precision,
                 cudaStream_t st) {
+  NvtxRange nv("S3TTMc");
   s3ttmc_reserve(t, R, packed, precision);
   ItemSet all;
   all.chunks = t.chunks.p;
@@ -588,6 +589,7 @@ static uint32_t host_band_count(size_t ybytes) {
 }
 
 void s3ttmc_host(TensorState &t, const void *U, uint32_t R, bool packed, void *Y, int precision) {
+  NvtxRange nv("S3TTMc (host buffers, row bands)");
   s3ttmc_reserve(t, R, packed, precision);
   const size_t es = precision == SYMPROP_FP64 ? 8 : 4;
   uint64_t cols = packed ? symsize(R, t.order - 1) : 1;

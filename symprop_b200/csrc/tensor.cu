@@ -154,6 +154,7 @@ static uint32_t row_order_items(const TensorState &t, std::vector<Chunk> &ch, st
 static bool heavier(const Chunk &a, const Chunk &b) { return (a.oe - a.ob) > (b.oe - b.ob); }
 
 void tensor_build(TensorState &t, const uint32_t *h_inds, const double *h_vals, bool on_device) {
+  NvtxRange nv("tensor build");
   const uint32_t N = t.order;
   const uint64_t nnz = t.nnz;
   cudaStream_t st = 0;

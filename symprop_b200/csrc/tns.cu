@@ -211,6 +211,7 @@ uint64_t read_header(const char *b, uint64_t len, uint32_t &order, uint32_t &dim
 // Parses the file text into device arrays (sorted tuples, values).
 void tns_parse_device(const char *h_bytes, uint64_t len, uint32_t &order, uint32_t &dim, uint64_t &nnz,
                       DBuf<uint32_t> &d_inds, DBuf<double> &d_vals) {
+  NvtxRange nv("tns parse");
   const uint64_t body = read_header(h_bytes, len, order, dim);
   if (order < 2 || order > (uint32_t)kMaxTnsOrder)
     fail(SYMPROP_ERR_ORDER, "order %u not supported (2..%d)", order, kMaxTnsOrder);

@@ -243,6 +243,7 @@ uint64_t sort_unique(DBuf<uint64_t> &words, uint64_t cnt, const KeyFmt &f, DBuf<
 }  // namespace
 
 void tree_build(TensorState &t) {
+  NvtxRange nv("CompressedDTree");
   if (t.tree) return;
   const uint32_t N = t.order;
   if (N < 2) fail(SYMPROP_ERR_ORDER, "order %u has no tree", N);

@@ -107,6 +107,7 @@ int hoevd_matrix_free(TensorState &t, cudaStream_t st, int r, double *U);
 constexpr int kHoevdDenseMax = 8192;
 
 int run_tucker(TensorState &t, const symprop_config &c, int alg, symprop_result &res) {
+  NvtxRange nv(alg == SYMPROP_HOOI ? "TuckerHOOI" : alg == SYMPROP_HOQRI ? "TuckerHOQRI" : "TuckerAltHOOI");
   const int n = (int)t.dim, N = (int)t.order, r = (int)c.rank;
   if (r < 1) fail(SYMPROP_ERR_INVALID, "rank must be positive");
   if (r > n) fail(SYMPROP_ERR_INVALID, "rank %d exceeds dim %d", r, n);
@@ -220,9 +221,11 @@ int run_tucker(TensorState &t, const symprop_config &c, int alg, symprop_result 
     // eigen-residual target relative to the largest eigenvalue: the FP32 /
     // split-BF16 Gram of the mixed phase resolves about 1e-6 of it
     const double eig_tol = mx ? 1e-5 : fp64_eig_tol;
+    nvtxRangePushA("regularize");
     tphase.start();
     regularize(st, U.p, n, r, c.delta);
     dense_ms += tphase.stop_ms();
+    nvtxRangePop();
 
     tphase.start();
     if (mx) {
@@ -233,6 +236,7 @@ int run_tucker(TensorState &t, const symprop_config &c, int alg, symprop_result 
     }
     s3_ms += tphase.stop_ms();
 
+    nvtxRangePushA("dense step");
     tphase.start();
     double rel_res = 0.0;
     if (alg == SYMPROP_HOOI || alg == SYMPROP_ALTHOOI) {
@@ -315,6 +319,7 @@ int run_tucker(TensorState &t, const symprop_config &c, int alg, symprop_result 
       cn2 = h[1];
     }
     dense_ms += tphase.stop_ms();
+    nvtxRangePop();
     if (mx && !gram_nn) {
       int herr = 0;
       SPB_CUDA(cudaMemcpy(&herr, gram_err.p, sizeof(int), cudaMemcpyDeviceToHost));
