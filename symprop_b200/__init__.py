@@ -17,7 +17,9 @@ from dataclasses import dataclass, field
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libsymprop_b200.so")
+# SYMPROP_B200_LIB selects another build of the library, e.g. the
+# bounds-checked libsymprop_b200_checked.so (make -C symprop_b200 checked)
+LIB_PATH = os.environ.get("SYMPROP_B200_LIB") or os.path.join(HERE, "libsymprop_b200.so")
 CLI_PATH = os.path.join(HERE, "symtucker")
 TTMC_PATH = os.path.join(HERE, "symtens_ttmc")
 TTMCTC_PATH = os.path.join(HERE, "s3ttmctc")

@@ -24,6 +24,7 @@
 #include <map>
 #include <mutex>
 
+#include "check.cuh"
 #include "s3ttmc_tiled.cuh"
 #include "s3ttmc_warp.cuh"
 #include "tensor.cuh"
@@ -175,6 +176,8 @@ struct RowParams {
   uint32_t desc_begin[kMaxL + 1];
   uint32_t desc_count[kMaxL + 1];
   uint32_t final_src[kMaxL];
+  uint64_t nown;  // bounds the checked build tests
+  uint32_t nrows, nslots;
 };
 
 template <typename T> struct Acc;
@@ -190,6 +193,9 @@ __global__ void __launch_bounds__(256, 1) s3ttmc_rows_kernel(const RowParams p) 
   extern __shared__ __align__(16) unsigned char smem[];
   const int tid = threadIdx.x, nt = blockDim.x;
   const Chunk ch = p.chunks[blockIdx.x];
+  if (!SPB_BOUND(ch.ob <= ch.oe && ch.oe <= p.nown && ch.row < p.nrows && (ch.slot == kDirect || ch.slot < p.nslots),
+                 301, blockIdx.x))
+    return;  // the whole CTA leaves (the chunk is the CTA's)
   const uint32_t R = p.R;
 
   uint32_t *sTab = reinterpret_cast<uint32_t *>(smem);
@@ -232,7 +238,8 @@ __global__ void __launch_bounds__(256, 1) s3ttmc_rows_kernel(const RowParams p) 
     const T c = own_c[o];
     for (uint32_t i = tid; i < L * R; i += nt) {
       uint32_t k = i / R, x = i - k * R;
-      T u = U[(uint64_t)S[k] * R + x];
+      const uint32_t id = S[k];
+      T u = SPB_BOUND(id < p.nrows, 302, id) ? U[(uint64_t)id * R + x] : T(0);
       sU[i] = u;
       sW[i] = c * u;
     }
@@ -319,9 +326,12 @@ __global__ void __launch_bounds__(256, 1) s3ttmc_rows_kernel(const RowParams p) 
 // warp order (deterministic)
 template <typename T>
 __global__ void __launch_bounds__(256) combine_kernel(const SplitRow *split, const double *partials,
-                                                      uint32_t mL, void *Yv, uint64_t ldy) {
+                                                      uint32_t mL, void *Yv, uint64_t ldy, uint32_t nrows,
+                                                      uint32_t nslots) {
   __shared__ double red[8][32];
   const SplitRow s = split[blockIdx.x];
+  if (!SPB_BOUND(s.row < nrows && s.slot_begin <= s.slot_end && s.slot_end <= nslots, 401, blockIdx.x))
+    return;  // the whole CTA leaves (the split row is the CTA's)
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const uint32_t q = blockIdx.y * 32 + lane;
   double a = 0.0;
@@ -374,6 +384,7 @@ __global__ void unpack_kernel(const T *packed, uint64_t rows, uint64_t m, uint32
     }
     start = q[j];
   }
+  if (!SPB_BOUND(order <= 16 && pos < m, 402, pos)) return;
   full[idx] = packed[r * m + pos];
 }
 
@@ -446,6 +457,7 @@ void unpack_rows(const void *dpacked, uint64_t rows, uint32_t dim, uint32_t orde
     unpack_kernel<float><<<grid, 256, 0, st>>>((const float *)dpacked, rows, m, dim, order, full,
                                                (float *)dfull);
   SPB_LAUNCH_CHECK();
+  spb_check_host(st, "unpack");
 }
 
 // One pass over a set of work items: writes the packed rows (or, when
@@ -515,6 +527,9 @@ static void s3ttmc_items(TensorState &t, const ItemSet &items, const void *dU, u
     rp.desc_count[d] = tb.level_desc_count[d];
   }
   for (uint32_t k = 0; k < L; ++k) rp.final_src[k] = tb.final_src[k];
+  rp.nown = t.nown;
+  rp.nrows = t.dim;
+  rp.nslots = t.nslots;
   const size_t smem = tb.smem_bytes[precision == SYMPROP_FP64 ? 0 : 1];
   if (smem > 227 * 1024)
     fail(SYMPROP_ERR_SIZE, "order %u rank %u needs %zu bytes of shared memory", t.order, R, smem);
@@ -523,6 +538,7 @@ static void s3ttmc_items(TensorState &t, const ItemSet &items, const void *dU, u
       dispatch_rows<double>(L, tb, rp, items.nchunks, smem, st);
     else
       dispatch_rows<float>(L, tb, rp, items.nchunks, smem, st);
+    spb_check_host(st, "S3TTMc rows kernel");
   }
   finish_rows(t, items, m, Ypk, packed, dY, R, L, precision, st);
 }
@@ -666,9 +682,11 @@ static void finish_rows(TensorState &t, const ItemSet &items, uint64_t m, void *
   if (items.nsplit) {
     dim3 grid(items.nsplit, (unsigned)((m + 31) / 32));
     if (precision == SYMPROP_FP64)
-      combine_kernel<double><<<grid, 256, 0, st>>>(items.split, t.partials.p, (uint32_t)m, Ypk, m);
+      combine_kernel<double><<<grid, 256, 0, st>>>(items.split, t.partials.p, (uint32_t)m, Ypk, m, t.dim,
+                                                   t.nslots);
     else
-      combine_kernel<float><<<grid, 256, 0, st>>>(items.split, t.partials.p, (uint32_t)m, Ypk, m);
+      combine_kernel<float><<<grid, 256, 0, st>>>(items.split, t.partials.p, (uint32_t)m, Ypk, m, t.dim,
+                                                  t.nslots);
     SPB_LAUNCH_CHECK();
   }
   if (!packed && items.rows) {
@@ -678,6 +696,7 @@ static void finish_rows(TensorState &t, const ItemSet &items, uint64_t m, void *
     unpack_rows((const char *)Ypk + (size_t)items.row0 * m * es, items.rows, R, L,
                 (char *)dY + (size_t)items.row0 * full * es, precision, st);
   }
+  spb_check_host(st, "S3TTMc combine / unpack");
 }
 
 static std::atomic<int> g_schedule{kScheduleAuto};

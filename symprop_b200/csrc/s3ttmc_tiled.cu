@@ -27,6 +27,7 @@
 #include <algorithm>
 #include <cstdlib>
 
+#include "check.cuh"
 #include "s3ttmc_tiled.cuh"
 
 namespace spb {
@@ -70,6 +71,8 @@ struct TiledParams {
   const uint32_t *lexidx;   // colex index at level L -> lexicographic packed index
   uint32_t ksz4;            // padded per-owner DP storage
   uint32_t BO, G;
+  uint64_t nown;            // bounds the checked build tests
+  uint32_t nrows, nslots;
 };
 
 template <typename T> struct Vec4;
@@ -96,6 +99,9 @@ __global__ void __launch_bounds__(kThreads, 2) s3ttmc_tiled_kernel(const TiledPa
   extern __shared__ __align__(16) unsigned char smem[];
   const int tid = threadIdx.x;
   const Chunk ch = p.chunks[blockIdx.x];
+  if (!SPB_BOUND(ch.ob <= ch.oe && ch.oe <= p.nown && ch.row < p.nrows && (ch.slot == kDirect || ch.slot < p.nslots),
+                 201, blockIdx.x))
+    return;  // the whole CTA leaves (the chunk is the CTA's)
   const uint32_t R = p.R, R4 = p.R4, BO = p.BO, G = p.G;
 
   // ---- shared memory carve
@@ -161,7 +167,10 @@ __global__ void __launch_bounds__(kThreads, 2) s3ttmc_tiled_kernel(const TiledPa
       while (o < nb) {
         const uint32_t i = o * per + k * R4 + x;
         T u = T(0);
-        if (x < R) u = U[(uint64_t)p.own_S[(ob + o) * p.sstride + k] * R + x];
+        if (x < R) {
+          const uint32_t id = p.own_S[(ob + o) * p.sstride + k];
+          if (SPB_BOUND(id < p.nrows, 202, id)) u = U[(uint64_t)id * R + x];
+        }
         sU[i] = u;
         sW[i] = own_c[ob + o] * u;
         x += dX;
@@ -290,6 +299,7 @@ __global__ void __launch_bounds__(kThreads, 2) s3ttmc_tiled_kernel(const TiledPa
         const uint32_t r = (uint32_t)tl[t].x + i;
         if (r >= cnt) continue;
         const uint32_t q = p.lexidx[base + r];
+        if (!SPB_BOUND(q < p.mL, 203, q)) continue;
         const T val = acc[t][i][c] - cmp[t][i][c];
         if (ch.slot == kDirect)
           reinterpret_cast<T *>(p.Y)[(uint64_t)ch.row * p.ldy + q] = val;
@@ -504,9 +514,13 @@ void tiled_launch(const TiledPlan &pl, const TensorState &t, const ItemSet &item
   tp.ksz4 = pl.ksz4;
   tp.BO = pl.BO[pi];
   tp.G = pl.G;
+  tp.nown = t.nown;
+  tp.nrows = t.dim;
+  tp.nslots = t.nslots;
   if (!items.nchunks) return;
   if (pi == 0) launch_tiled_l<double>(pl.L, pl.NT, tp, items.nchunks, pl.smem[0], st);
   else launch_tiled_l<float>(pl.L, pl.NT, tp, items.nchunks, pl.smem[1], st);
+  spb_check_host(st, "S3TTMc tiled kernel");
 }
 
 }  // namespace spb

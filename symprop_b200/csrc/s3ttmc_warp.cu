@@ -32,6 +32,7 @@
 #include <algorithm>
 #include <utility>
 
+#include "check.cuh"
 #include "s3ttmc_warp.cuh"
 
 namespace spb {
@@ -72,6 +73,9 @@ struct WarpParams {
   const uint4 *rowoff;               // per tile: lex offset - j of its 4 rows, or kPadRow
   uint32_t ntiles;
   uint32_t wsz;                      // per-warp staging elements: 2*L*R4 + ksz4
+  uint32_t ksz;                      // elements of the level tensors (levels 2..L-2) in a staging area
+  uint64_t nown;                     // bounds the checked build tests
+  uint32_t nrows, nslots;
 };
 
 template <typename T> __device__ __forceinline__ void ld4(const T *p, T (&v)[4]) {
@@ -217,6 +221,11 @@ __device__ __forceinline__ void dp_level(const WarpParams &p, const SmemTables &
   T *dst = sK + p.lvl_off[D];
   for (uint32_t e = tid; e < md; e += nthr) {
     const uint32_t j = jt[e], r = e - stt[j];
+    if (!SPB_BOUND(j < p.R && p.lvl_off[D] + (uint32_t)(nmasks(L, D) - 1) * p.mstr[D] + prow<T>(e) < p.ksz &&
+                       (D == 2 ? (uint32_t)(NS - 1) * R4 + r < (uint32_t)L * R4
+                               : p.lvl_off[D - 1] + (uint32_t)(NS - 1) * sstr + prow<T>(r) < p.ksz),
+                   106, e))
+      continue;
     T uj[L], src[NS];
 #pragma unroll
     for (int k = 0; k < L; ++k) uj[k] = sU[k * R4 + j];
@@ -249,6 +258,7 @@ __device__ __forceinline__ void tile_step(const WarpParams &p, const T *sU, cons
   for (int i = 0; i < NTL; ++i) {
     if (!live[i]) continue;
     const uint32_t r0 = (uint32_t)tl[i].x, jt = (uint32_t)tl[i].y, x0 = (uint32_t)tl[i].z;
+    if (!SPB_BOUND(x0 + 3 < R4 && jt < p.R, 105, ((uint64_t)x0 << 32) | jt)) continue;
     T w[L][4], uj[L], A[L][4];
 #pragma unroll
     for (int k = 0; k < L; ++k) ld4(sW + k * R4 + x0, w[k]);
@@ -270,9 +280,12 @@ __device__ __forceinline__ void tile_step(const WarpParams &p, const T *sU, cons
 #pragma unroll
         for (int t = k + 1; t < L; ++t) {
           const uint32_t s = p.pair_src[pidx(k, t, L)];
-          T kv[4];
-          if constexpr (L == 3) ld4(sU + (s & 0xffu) * R4 + r0, kv);
-          else ld4(sK + s + prow<T>(r0), kv);
+          T kv[4] = {T(0), T(0), T(0), T(0)};
+          if constexpr (L == 3) {
+            if (SPB_BOUND((s & 0xffu) * R4 + r0 + 3 < (uint32_t)L * R4, 104, r0)) ld4(sU + (s & 0xffu) * R4 + r0, kv);
+          } else {
+            if (SPB_BOUND(s + prow<T>(r0 + 3) < p.ksz, 104, r0)) ld4(sK + s + prow<T>(r0), kv);
+          }
           if constexpr (sizeof(T) == 4) {  // row pairs on the paired FP32 pipe
 #pragma unroll
             for (int h = 0; h < 4; h += 2) {
@@ -364,6 +377,7 @@ __device__ __forceinline__ void write_tiles(const WarpParams &p, const Chunk &ch
         const uint32_t x = (uint32_t)tl[i].z + cc;
         if (x >= p.R || x < (uint32_t)tl[i].y) continue;
         const uint32_t qo = rof[q] + x;
+        if (!SPB_BOUND(qo < p.mL, 103, qo)) continue;
         if (ch.slot == kDirect) Yrow[qo] = acc[i][q][cc];
         else Prow[qo] = (double)acc[i][q][cc];
       }
@@ -388,6 +402,9 @@ __global__ void __launch_bounds__(kThreads, (min_blocks<T, NTL>())) s3ttmc_warp_
   const uint32_t item = blockIdx.x * (uint32_t)kWarps + (uint32_t)warp;
   if (item >= p.nchunks) return;
   const Chunk ch = p.chunks[item];
+  if (!SPB_BOUND(ch.ob <= ch.oe && ch.oe <= p.nown && ch.row < p.nrows && (ch.slot == kDirect || ch.slot < p.nslots),
+                 101, item))
+    return;
 
   // this lane's tiles: 4 consecutive rows r0..r0+3 of block j (all with last
   // index j) times columns x0..x0+3
@@ -432,7 +449,8 @@ __global__ void __launch_bounds__(kThreads, (min_blocks<T, NTL>())) s3ttmc_warp_
   // and coefficient of owner o+1 and the ids of owner o+2 are in flight.
   // Lane k < L holds id k of an owner; the staging lanes fetch it by shuffle.
   auto load_ids = [&](uint64_t o) -> uint32_t {
-    return (o < ch.oe && lane < L) ? p.own_S[o * p.sstride + (uint32_t)lane] : 0u;
+    const uint32_t id = (o < ch.oe && lane < L) ? p.own_S[o * p.sstride + (uint32_t)lane] : 0u;
+    return SPB_BOUND(id < p.nrows, 102, id) ? id : 0u;
   };
   auto load_rows = [&](uint32_t idv, T (&u)[kP]) {
 #pragma unroll
@@ -516,6 +534,9 @@ __global__ void __launch_bounds__(kThreads, (min_blocks<T, NTL>())) s3ttmc_team_
   T *sBuf = reinterpret_cast<T *>(tb.rest);  // kNB x wsz
   float2 *sK2 = reinterpret_cast<float2 *>(sBuf + (size_t)kNB * p.wsz);
   const Chunk ch = p.chunks[blockIdx.x];
+  if (!SPB_BOUND(ch.ob <= ch.oe && ch.oe <= p.nown && ch.row < p.nrows && (ch.slot == kDirect || ch.slot < p.nslots),
+                 101, blockIdx.x))
+    return;  // the whole CTA leaves (the chunk is the CTA's)
 
   int4 tl[NTL];
   bool live[NTL];
@@ -553,7 +574,8 @@ __global__ void __launch_bounds__(kThreads, (min_blocks<T, NTL>())) s3ttmc_team_
   const uint32_t sq = stager ? tid / LR4 : 0u, se = stager ? tid - sq * LR4 : 0u;
   const uint32_t sk = se / R4, sx = se - sk * R4;
   auto load_id = [&](uint64_t o) -> uint32_t {
-    return (stager && o < nown) ? p.own_S[(ch.ob + o) * p.sstride + sk] : 0u;
+    const uint32_t id = (stager && o < nown) ? p.own_S[(ch.ob + o) * p.sstride + sk] : 0u;
+    return SPB_BOUND(id < p.nrows, 102, id) ? id : 0u;
   };
   T u_n = T(0), c_n = T(0);
   if (stager && sq < nown) {
@@ -842,8 +864,13 @@ void warp_launch(const WarpPlan &pl, const TensorState &t, const ItemSet &items,
   wp.rowoff = pl.rowoff.p;
   wp.ntiles = pl.ntiles;
   wp.wsz = pl.wsz;
+  wp.ksz = pl.ksz4;
+  wp.nown = t.nown;
+  wp.nrows = t.dim;
+  wp.nslots = t.nslots;
   if (pi == 0) launch_w_l<double>(pl.L, pl.NTL, pl.team, wp, items.nchunks, pl.smem[0], st);
   else launch_w_l<float>(pl.L, pl.NTL, pl.team, wp, items.nchunks, pl.smem[1], st);
+  spb_check_host(st, pl.team ? "S3TTMc team kernel" : "S3TTMc warp kernel");
 }
 
 }  // namespace spb
