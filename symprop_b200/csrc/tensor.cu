@@ -11,7 +11,8 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
-#include <numeric>
+#include <chrono>
+#include <cstdlib>
 
 #include "tensor.cuh"
 
@@ -20,6 +21,11 @@ namespace spb {
 namespace {
 
 constexpr int kMaxOrder = 16;
+
+__global__ void iota_kernel(uint32_t *p, uint64_t n) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    p[i] = (uint32_t)i;
+}
 
 __global__ void validate_kernel(const uint32_t *inds, uint64_t nnz, uint32_t order,
                                 uint32_t dim, uint32_t *inds0, int *bad) {
@@ -151,10 +157,30 @@ static uint32_t row_order_items(const TensorState &t, std::vector<Chunk> &ch, st
   return slot;
 }
 
-static bool heavier(const Chunk &a, const Chunk &b) { return (a.oe - a.ob) > (b.oe - b.ob); }
+// Stable sort of ch[b, e) by owner count, heaviest first: a counting sort,
+// since no chunk holds more than max_owners owners.
+static void sort_heaviest_first(std::vector<Chunk> &ch, size_t b, size_t e, uint64_t max_owners) {
+  std::vector<size_t> start(max_owners + 2, 0);
+  for (size_t i = b; i < e; ++i) ++start[max_owners - (ch[i].oe - ch[i].ob) + 1];
+  for (size_t k = 1; k < start.size(); ++k) start[k] += start[k - 1];
+  std::vector<Chunk> out(e - b);
+  for (size_t i = b; i < e; ++i) out[start[max_owners - (ch[i].oe - ch[i].ob)]++] = ch[i];
+  std::copy(out.begin(), out.end(), ch.begin() + (std::ptrdiff_t)b);
+}
 
 void tensor_build(TensorState &t, const uint32_t *h_inds, const double *h_vals, bool on_device) {
   NvtxRange nv("tensor build");
+  // SPB_TRACE_BUILD=1 prints the time of each phase (with a device sync)
+  const bool trace = std::getenv("SPB_TRACE_BUILD") != nullptr;
+  auto tlast = std::chrono::steady_clock::now();
+  auto mark = [&](const char *phase) {
+    if (!trace) return;
+    SPB_CUDA(cudaDeviceSynchronize());
+    const auto now = std::chrono::steady_clock::now();
+    std::fprintf(stderr, "tensor build: %-28s %8.2f ms\n", phase,
+                 std::chrono::duration<double, std::milli>(now - tlast).count());
+    tlast = now;
+  };
   const uint32_t N = t.order;
   const uint64_t nnz = t.nnz;
   cudaStream_t st = 0;
@@ -168,6 +194,7 @@ void tensor_build(TensorState &t, const uint32_t *h_inds, const double *h_vals, 
     SPB_CUDA(cudaMemcpy(raw.p, h_inds, nnz * N * sizeof(uint32_t), kind));
     SPB_CUDA(cudaMemcpy(t.vals.p, h_vals, nnz * sizeof(double), kind));
   }
+  mark("allocate + copy tuples in");
   DBuf<int> bad(1);
   SPB_CUDA(cudaMemset(bad.p, 0, sizeof(int)));
   if (nnz) {
@@ -179,6 +206,7 @@ void tensor_build(TensorState &t, const uint32_t *h_inds, const double *h_vals, 
   if (hbad & 1) fail(SYMPROP_ERR_INVALID, "index out of range [1, %u]", t.dim);
   if (hbad & 2) fail(SYMPROP_ERR_INVALID, "index tuple not sorted ascending");
   raw.release();
+  mark("validate");
 
   // owners per tuple + ||X||^2 terms
   DBuf<uint32_t> cnt(nnz + 1), off(nnz + 1);
@@ -207,6 +235,7 @@ void tensor_build(TensorState &t, const uint32_t *h_inds, const double *h_vals, 
   SPB_CUDA(cudaMemcpy(&total, off.p + nnz, sizeof(uint32_t), cudaMemcpyDeviceToHost));
   SPB_CUDA(cudaMemcpy(&nsq, dsum.p, sizeof(double), cudaMemcpyDeviceToHost));
   t.norm = std::sqrt(nsq);
+  mark("count owners, norm");
   t.nown = total;
   t.sstride = ((N - 1) + 3) / 4 * 4;
   if (N - 1 == 0) t.sstride = 4;
@@ -222,13 +251,12 @@ void tensor_build(TensorState &t, const uint32_t *h_inds, const double *h_vals, 
   cnt.release();
   off.release();
   normsq.release();
+  mark("emit owners");
 
   // stable radix sort of owners by row
   DBuf<uint32_t> rows_sorted(t.nown), perm_in(t.nown), perm(t.nown);
   if (t.nown) {
-    std::vector<uint32_t> iota(t.nown);
-    std::iota(iota.begin(), iota.end(), 0u);
-    SPB_CUDA(cudaMemcpy(perm_in.p, iota.data(), t.nown * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    device_iota(perm_in.p, t.nown, st);
     int end_bit = bits_for(t.dim);
     size_t tmp = 0;
     SPB_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, own_row.p, rows_sorted.p, perm_in.p,
@@ -237,6 +265,7 @@ void tensor_build(TensorState &t, const uint32_t *h_inds, const double *h_vals, 
     SPB_CUDA(cub::DeviceRadixSort::SortPairs(work.p, tmp, own_row.p, rows_sorted.p, perm_in.p,
                                              perm.p, t.nown, 0, end_bit, st));
   }
+  mark("sort owners by row");
   t.own_S.alloc(t.nown * t.sstride);
   t.own_c64.alloc(t.nown);
   t.own_c32.alloc(t.nown);
@@ -253,6 +282,7 @@ void tensor_build(TensorState &t, const uint32_t *h_inds, const double *h_vals, 
   t.h_row_ptr.resize((size_t)t.dim + 1);
   SPB_CUDA(cudaMemcpy(t.h_row_ptr.data(), t.row_ptr.p, ((size_t)t.dim + 1) * sizeof(uint64_t),
                       cudaMemcpyDeviceToHost));
+  mark("gather owners, row pointers");
 
   // Work items: rows with more than chunk_owners owners are cut into slices
   // whose partial sums a second kernel adds in a fixed order.
@@ -263,7 +293,7 @@ void tensor_build(TensorState &t, const uint32_t *h_inds, const double *h_vals, 
   std::vector<Chunk> ch;
   std::vector<SplitRow> sp;
   const uint32_t slot = row_order_items(t, ch, sp);
-  std::stable_sort(ch.begin(), ch.end(), heavier);
+  sort_heaviest_first(ch, 0, ch.size(), co);
   t.nchunks = (uint32_t)ch.size();
   t.nheavy = 0;
   while (t.nheavy < t.nchunks && ch[t.nheavy].oe - ch[t.nheavy].ob > kLightOwners) ++t.nheavy;
@@ -277,6 +307,13 @@ void tensor_build(TensorState &t, const uint32_t *h_inds, const double *h_vals, 
     SPB_CUDA(cudaMemcpy(t.split.p, sp.data(), sp.size() * sizeof(SplitRow), cudaMemcpyHostToDevice));
   t.bands.reset();
   SPB_CUDA(cudaDeviceSynchronize());
+  mark("work items (host) + upload");
+}
+
+void device_iota(uint32_t *p, uint64_t n, cudaStream_t st) {
+  if (!n) return;
+  iota_kernel<<<(unsigned)std::min<uint64_t>((n + 255) / 256, 148ull * 64), 256, 0, st>>>(p, n);
+  SPB_LAUNCH_CHECK();
 }
 
 const RowBands &row_bands(TensorState &t, uint32_t nb) {
@@ -300,8 +337,7 @@ const RowBands &row_bands(TensorState &t, uint32_t nb) {
                                                [](const SplitRow &c, uint32_t v) { return c.row < v; }) -
                               sp.begin());
   }
-  for (uint32_t k = 0; k < nb; ++k)
-    std::stable_sort(ch.begin() + b->chunk0[k], ch.begin() + b->chunk0[k + 1], heavier);
+  for (uint32_t k = 0; k < nb; ++k) sort_heaviest_first(ch, b->chunk0[k], b->chunk0[k + 1], t.chunk_owners);
   b->chunks.alloc(ch.size());
   if (!ch.empty())
     SPB_CUDA(cudaMemcpy(b->chunks.p, ch.data(), ch.size() * sizeof(Chunk), cudaMemcpyHostToDevice));

@@ -144,6 +144,8 @@ void tree_build(TensorState &t);
 // tensor.cu
 // inds/vals in host memory, or in device memory when on_device is set
 void tensor_build(TensorState &t, const uint32_t *inds, const double *vals, bool on_device = false);
+// p[i] = i, i < n (permutation seeds of the radix sorts)
+void device_iota(uint32_t *p, uint64_t n, cudaStream_t stream);
 // the work items in nb row bands (built on first use, kept for the next call)
 const RowBands &row_bands(TensorState &t, uint32_t nb);
 

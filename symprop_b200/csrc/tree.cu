@@ -21,7 +21,6 @@
 // lexicographic order.
 #include <cub/cub.cuh>
 
-#include <numeric>
 
 #include "tensor.cuh"
 
@@ -195,11 +194,7 @@ uint64_t sort_unique(DBuf<uint64_t> &words, uint64_t cnt, const KeyFmt &f, DBuf<
                      DBuf<uint64_t> &nodes, DBuf<uint64_t> *seg_start) {
   cudaStream_t st = 0;
   perm.alloc(cnt);
-  {
-    std::vector<uint32_t> iota(cnt);
-    std::iota(iota.begin(), iota.end(), 0u);
-    if (cnt) SPB_CUDA(cudaMemcpy(perm.p, iota.data(), cnt * 4, cudaMemcpyHostToDevice));
-  }
+  device_iota(perm.p, cnt, st);
   DBuf<uint64_t> kin(cnt), kout(cnt);
   DBuf<uint32_t> pout(cnt);
   size_t tmp = 0;
