@@ -7,7 +7,7 @@ Every numeric step runs in this package's CUDA kernels through the C ABI
 symprop_mlp_backward, symprop_projector_loss, symprop_adam_step,
 symprop_ws_predict); torch only allocates device buffers.  Labels are the
 converged factors of this package's own FP64 GPU HOOI on seeded synthetic
-tensors; plain random-start HOOI stays the fallback and the judge.
+tensors; plain random-start HOOI stays the fallback and the reference point.
 """
 from __future__ import annotations
 

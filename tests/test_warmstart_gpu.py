@@ -81,7 +81,7 @@ def test_trained_network_gains_over_random_start(gpu):
     lrn = np.mean([r["learned_iters"] for r in rows])
     assert lrn < rnd, rows
     # HOOI is non-convex: each start may settle on a different fixed point, so
-    # the objective is judged on average over the held-out tensors
+    # the objective is compared on average over the held-out tensors
     e_rnd = np.mean([r["random_error"] for r in rows])
     e_lrn = np.mean([r["learned_error"] for r in rows])
     assert e_lrn <= e_rnd + 1e-4, (e_lrn, e_rnd)
