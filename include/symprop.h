@@ -81,6 +81,17 @@ int symprop_tensor_destroy(symprop_tensor *t);
  * offset instead of a silently shortened tensor.  Orders 2..8. */
 int symprop_tensor_load_tns(const char *path, symprop_tensor **out);
 
+/* Binary tuple files (SPT1; this library's companion to .tns, which the
+ * reference reads as text only).  Layout, little endian: "SPT1", u32 order,
+ * u32 dim, u32 0, u64 nnz, then nnz*order u32 ids (1-based, each tuple
+ * ascending) and nnz f64 values.  load_spt builds the same tensor as
+ * SpSymtensor(dim, order, ids, values) with no text to parse; a file whose
+ * size disagrees with its header, or an id outside [1, dim] or an unsorted
+ * tuple, is SYMPROP_ERR_INVALID; orders 2..8 (SYMPROP_ERR_ORDER otherwise).
+ * save_spt writes a tensor's tuples and values in that layout. */
+int symprop_tensor_load_spt(const char *path, symprop_tensor **out);
+int symprop_tensor_save_spt(const symprop_tensor *t, const char *path);
+
 /* Copies the tensor's sorted tuples (nnz*order uint32, 1-based) and values
  * (nnz) to host arrays; either pointer may be NULL.
  * SpSymtensor::unnz_inds / unnzs (include/detail/sparse/spsymtensor.hpp:35-37). */

@@ -256,6 +256,20 @@ class SpSymtensor {  // include/detail/sparse/spsymtensor.hpp:24-65
     check_status(symprop_tensor_load_tns(path.c_str(), &t));
     return SpSymtensor(t);
   }
+  // binary SPT1 tuple file (symprop_tensor_load_spt / save_spt)
+  static SpSymtensor load_spt(const std::string &path) {
+    symprop_tensor *t = nullptr;
+    check_status(symprop_tensor_load_spt(path.c_str(), &t));
+    return SpSymtensor(t);
+  }
+  void save_spt(const std::string &path) const { check_status(symprop_tensor_save_spt(_t.get(), path.c_str())); }
+  // a file that starts with "SPT1" is binary, anything else .tns text
+  static bool is_spt(const std::string &path) {
+    std::ifstream f(path, std::ios::binary);
+    char m[4] = {0, 0, 0, 0};
+    return f.read(m, 4) && m[0] == 'S' && m[1] == 'P' && m[2] == 'T' && m[3] == '1';
+  }
+  static SpSymtensor load(const std::string &path) { return is_spt(path) ? load_spt(path) : load_tns(path); }
 
   order_t order() const { return _order; }
   dim_t dim() const { return _dim; }

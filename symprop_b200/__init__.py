@@ -101,6 +101,8 @@ def lib():
         "symprop_gram_device_noalloc": (_I, [_P, _U64, _U32, _P, _P, _P]),
         "symprop_tensor_load_tns": (_I, [ctypes.c_char_p, ctypes.POINTER(_P)]),
         "symprop_tensor_copy_nonzeros": (_I, [_P, _P, _P]),
+        "symprop_tensor_load_spt": (_I, [ctypes.c_char_p, ctypes.POINTER(_P)]),
+        "symprop_tensor_save_spt": (_I, [_P, ctypes.c_char_p]),
         "symprop_gemmtn": (_I, [_P, _P, _P, _U64, _U64, _U64]),
         "symprop_symgemm": (_I, [_P, _P, _P, _P, _U64, _U64, _U64]),
         "symprop_symsyrk": (_I, [_P, _P, _P, _U64, _U64]),
@@ -125,7 +127,8 @@ def exported_symbols() -> list[str]:
         "symprop_tree_copy_owners", "symprop_s3ttmc", "symprop_s3ttmc_device", "symprop_s3ttmc_launches",
         "symprop_symtens_size", "symprop_symtens_coeff", "symprop_unpack_rows_device", "symprop_tucker",
         "symprop_write_decomp", "symprop_gram_device", "symprop_s3ttmc_schedule",
-        "symprop_tensor_load_tns", "symprop_tensor_copy_nonzeros",
+        "symprop_tensor_load_tns", "symprop_tensor_copy_nonzeros", "symprop_tensor_load_spt",
+        "symprop_tensor_save_spt",
         "symprop_gemmtn", "symprop_symgemm", "symprop_symsyrk", "symprop_qr", "symprop_syevd", "symprop_leftsvd",
     ]
 
@@ -262,9 +265,22 @@ class SpSymtensor:
     def load_tns(cls, path: str) -> "SpSymtensor":
         """SymtensLoader + SpSymtensor with the .tns text parsed on the device
         (symprop_tensor_load_tns)."""
+        return cls._from_file(lib().symprop_tensor_load_tns, path)
+
+    @classmethod
+    def load_spt(cls, path: str) -> "SpSymtensor":
+        """A binary SPT1 tuple file (symprop_tensor_load_spt; layout in
+        include/symprop.h and synth.write_spt)."""
+        return cls._from_file(lib().symprop_tensor_load_spt, path)
+
+    def save_spt(self, path: str) -> None:
+        _check(lib().symprop_tensor_save_spt(self._h, os.fsencode(path)))
+
+    @classmethod
+    def _from_file(cls, loader, path: str) -> "SpSymtensor":
         self = cls.__new__(cls)
         h = _P()
-        _check(lib().symprop_tensor_load_tns(os.fsencode(path), ctypes.byref(h)))
+        _check(loader(os.fsencode(path), ctypes.byref(h)))
         self._h = h
         o, d, z, n = _U32(0), _U32(0), _U64(0), _D(0)
         _check(lib().symprop_tensor_order(h, ctypes.byref(o)))

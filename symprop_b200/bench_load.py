@@ -1,6 +1,8 @@
 """Time .tns ingest: the reference's SymtensLoader (host iostream, timed by
 oracle/_ref/ref_probe when that build is present) against
-symprop_tensor_load_tns (file read + device tokenise/parse + tensor build).
+symprop_tensor_load_tns (file read + device tokenise/parse + tensor build)
+and against symprop_tensor_load_spt (the same tuples as a binary SPT1 file:
+file read + tensor build).
 
     python -m symprop_b200.bench_load --workload s3ttmc_order4_zipf
 
@@ -47,6 +49,16 @@ def main():
         Y = SpSymtensor(n, order, t, v)
         build_ms = (time.perf_counter() - t0) * 1e3
         Y.close()
+        spt = os.path.join(d, "x.spt")
+        synth.write_spt(spt, order, n, t, v)
+        spt_size = os.path.getsize(spt)
+        spt_ms = []
+        for _ in range(a.reps):
+            t0 = time.perf_counter()
+            Z = SpSymtensor.load_spt(spt)
+            spt_ms.append((time.perf_counter() - t0) * 1e3)
+            assert Z.size() == t.shape[0]
+            Z.close()
         ref = None
         probe = os.path.join(ROOT, "oracle", "_ref", "ref_probe")
         if os.path.exists(probe):
@@ -56,6 +68,7 @@ def main():
     print(json.dumps({"workload": a.workload, "scale": a.scale, "nnz": int(t.shape[0]), "order": order,
                       "file_mb": round(size / 1e6, 1), "device_load_ms": round(min(dev), 1),
                       "of_which_tensor_build_ms": round(build_ms, 1),
+                      "spt_file_mb": round(spt_size / 1e6, 1), "spt_load_ms": round(min(spt_ms), 1),
                       "reference_loader_ms": ref,
                       "reference_loader_note": "host iostream parse only (tree build not included)"}))
 

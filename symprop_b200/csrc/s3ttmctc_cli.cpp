@@ -36,7 +36,7 @@ int main(int argc, char **argv) {
   }
   try {
     auto t1 = std::chrono::high_resolution_clock::now();
-    SpSymtensor symtens = SpSymtensor::load_tns(input_file);
+    SpSymtensor symtens = SpSymtensor::load(input_file);  // .tns text, or a binary SPT1 file
     auto t2 = std::chrono::high_resolution_clock::now();
     std::cout << "Insertion time: " << std::chrono::duration_cast<std::chrono::milliseconds>(t2 - t1).count()
               << " ms" << std::endl;

@@ -6,7 +6,8 @@
 // build: -p fp64|mixed (precision; default fp64 = the reference's FP64
 // arithmetic), -q (suppress per-iteration lines).  "Insertion time" covers
 // the device parse of the file and the tensor build (the reference parses
-// on the host before its timer starts).
+// on the host before its timer starts).  -f also takes a binary SPT1 tuple
+// file (symprop_tensor_load_spt), recognised by its first four bytes.
 #include <chrono>
 #include <cstring>
 #include <fstream>
@@ -95,7 +96,9 @@ int main(int argc, char **argv) {
     // through SymtensLoader, whose stream semantics and messages decide.
     auto t1 = std::chrono::high_resolution_clock::now();
     std::optional<SpSymtensor> loaded;
-    if (std::ifstream(input->filePath).is_open()) {
+    if (SpSymtensor::is_spt(input->filePath)) {  // binary SPT1 tuple file: no text rules apply
+      loaded.emplace(SpSymtensor::load_spt(input->filePath));
+    } else if (std::ifstream(input->filePath).is_open()) {
       try {
         loaded.emplace(SpSymtensor::load_tns(input->filePath));
       } catch (const std::runtime_error &) {

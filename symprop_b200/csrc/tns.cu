@@ -357,6 +357,81 @@ int symprop_tensor_load_tns(const char *path, symprop_tensor **out) {
   });
 }
 
+int symprop_tensor_load_spt(const char *path, symprop_tensor **out) {
+  return guard([&] {
+    if (!path || !out) fail(SYMPROP_ERR_INVALID, "null argument");
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+      cudaGetLastError();
+      fail(SYMPROP_ERR_NODEVICE, "no CUDA device visible");
+    }
+    std::FILE *f = std::fopen(path, "rb");
+    if (!f) fail(SYMPROP_ERR_INVALID, "cannot open %s", path);
+    std::unique_ptr<std::FILE, int (*)(std::FILE *)> fh(f, std::fclose);
+    unsigned char head[24];
+    if (std::fread(head, 1, sizeof head, f) != sizeof head || std::memcmp(head, "SPT1", 4) != 0)
+      fail(SYMPROP_ERR_INVALID, "%s: not an SPT1 tuple file", path);
+    uint32_t order = 0, dim = 0;
+    uint64_t nnz = 0;
+    std::memcpy(&order, head + 4, 4);
+    std::memcpy(&dim, head + 8, 4);
+    std::memcpy(&nnz, head + 16, 8);
+    if (order < 2 || order > 8) fail(SYMPROP_ERR_ORDER, "order %u not supported (2..8)", order);
+    if (dim == 0) fail(SYMPROP_ERR_INVALID, "dim must be positive");
+    if (nnz >= (1ull << 32) / order) fail(SYMPROP_ERR_SIZE, "nnz*order must be below 2^32");
+    std::fseek(f, 0, SEEK_END);
+    const long sz = std::ftell(f);
+    const uint64_t ibytes = nnz * order * 4, vbytes = nnz * 8;
+    if (sz < 0 || (uint64_t)sz != sizeof head + ibytes + vbytes)
+      fail(SYMPROP_ERR_INVALID, "%s: %ld bytes, the header announces %llu", path, sz,
+           (unsigned long long)(sizeof head + ibytes + vbytes));
+    std::fseek(f, (long)sizeof head, SEEK_SET);
+    char *buf = nullptr;
+    if (ibytes + vbytes && cudaMallocHost(&buf, ibytes + vbytes) != cudaSuccess) {
+      cudaGetLastError();
+      fail(SYMPROP_ERR_OOM, "pinned host buffer of %llu bytes", (unsigned long long)(ibytes + vbytes));
+    }
+    std::unique_ptr<char, void (*)(char *)> hold(buf, [](char *p) { if (p) cudaFreeHost(p); });
+    if (ibytes + vbytes && std::fread(buf, 1, ibytes + vbytes, f) != ibytes + vbytes)
+      fail(SYMPROP_ERR_INVALID, "short read of %s", path);
+    DBuf<uint32_t> inds(nnz * order);
+    DBuf<double> vals(nnz);
+    if (nnz) {
+      SPB_CUDA(cudaMemcpy(inds.p, buf, ibytes, cudaMemcpyHostToDevice));
+      SPB_CUDA(cudaMemcpy(vals.p, buf + ibytes, vbytes, cudaMemcpyHostToDevice));
+    }
+    auto t = std::make_unique<symprop_tensor>();
+    SPB_CUDA(cudaGetDevice(&t->s.device));
+    t->s.order = order;
+    t->s.dim = dim;
+    t->s.nnz = nnz;
+    tensor_build(t->s, inds.p, vals.p, true);  // checks every id against [1, dim] and the tuple order
+    *out = t.release();
+  });
+}
+
+int symprop_tensor_save_spt(const symprop_tensor *t, const char *path) {
+  return guard([&] {
+    if (!t || !path) fail(SYMPROP_ERR_INVALID, "null argument");
+    const uint32_t order = t->s.order, dim = t->s.dim, zero = 0;
+    const uint64_t nnz = t->s.nnz;
+    std::vector<uint32_t> inds(nnz * order);
+    std::vector<double> vals(nnz);
+    if (nnz && symprop_tensor_copy_nonzeros(t, inds.data(), vals.data()) != SYMPROP_OK)
+      fail(SYMPROP_ERR_CUDA, "copying the nonzeros out failed");
+    std::FILE *f = std::fopen(path, "wb");
+    if (!f) fail(SYMPROP_ERR_INVALID, "cannot create %s", path);
+    std::unique_ptr<std::FILE, int (*)(std::FILE *)> fh(f, std::fclose);
+    bool ok = std::fwrite("SPT1", 1, 4, f) == 4 && std::fwrite(&order, 4, 1, f) == 1 &&
+              std::fwrite(&dim, 4, 1, f) == 1 && std::fwrite(&zero, 4, 1, f) == 1 && std::fwrite(&nnz, 8, 1, f) == 1;
+    if (ok && nnz)
+      ok = std::fwrite(inds.data(), 4, inds.size(), f) == inds.size() &&
+           std::fwrite(vals.data(), 8, vals.size(), f) == vals.size();
+    if (!ok) fail(SYMPROP_ERR_INVALID, "short write of %s", path);
+  });
+}
+
 int symprop_tensor_copy_nonzeros(const symprop_tensor *t, uint32_t *inds, double *vals) {
   return guard([&] {
     if (!t) fail(SYMPROP_ERR_INVALID, "null tensor");
