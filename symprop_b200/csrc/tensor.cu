@@ -305,7 +305,7 @@ void tensor_build(TensorState &t, const uint32_t *h_inds, const double *h_vals, 
   t.split.alloc(sp.size());
   if (!sp.empty())
     SPB_CUDA(cudaMemcpy(t.split.p, sp.data(), sp.size() * sizeof(SplitRow), cudaMemcpyHostToDevice));
-  t.bands.reset();
+  t.bands.clear();
   SPB_CUDA(cudaDeviceSynchronize());
   mark("work items (host) + upload");
 }
@@ -318,7 +318,8 @@ void device_iota(uint32_t *p, uint64_t n, cudaStream_t st) {
 
 const RowBands &row_bands(TensorState &t, uint32_t nb) {
   nb = std::max<uint32_t>(1, std::min<uint32_t>(nb, std::max<uint32_t>(t.dim, 1)));
-  if (t.bands && t.bands->nb == nb) return *t.bands;
+  auto found = t.bands.find(nb);
+  if (found != t.bands.end()) return *found->second;
   auto b = std::make_unique<RowBands>();
   b->nb = nb;
   std::vector<Chunk> ch;
@@ -344,8 +345,7 @@ const RowBands &row_bands(TensorState &t, uint32_t nb) {
   b->split.alloc(sp.size());
   if (!sp.empty())
     SPB_CUDA(cudaMemcpy(b->split.p, sp.data(), sp.size() * sizeof(SplitRow), cudaMemcpyHostToDevice));
-  t.bands = std::move(b);
-  return *t.bands;
+  return *(t.bands[nb] = std::move(b));
 }
 
 }  // namespace spb

@@ -127,7 +127,7 @@ struct TensorState {
   std::map<uint32_t, std::shared_ptr<TiledPlan>> tiled;      // by R
   std::map<uint32_t, std::shared_ptr<WarpPlan>> warp;        // by R
   std::unique_ptr<TreeLevels> tree;
-  std::unique_ptr<RowBands> bands;
+  std::map<uint32_t, std::unique_ptr<RowBands>> bands;  // by band count
 };
 
 // s3ttmc.cu
@@ -146,7 +146,7 @@ void tree_build(TensorState &t);
 void tensor_build(TensorState &t, const uint32_t *inds, const double *vals, bool on_device = false);
 // p[i] = i, i < n (permutation seeds of the radix sorts)
 void device_iota(uint32_t *p, uint64_t n, cudaStream_t stream);
-// the work items in nb row bands (built on first use, kept for the next call)
+// the work items in nb row bands (built on first use, kept for later calls)
 const RowBands &row_bands(TensorState &t, uint32_t nb);
 
 }  // namespace spb
