@@ -18,8 +18,11 @@
 // or large exponents) are listed by the kernel and converted on the host
 // with strtod, which the reference's stream extraction also uses.
 #include <cub/cub.cuh>
+#include <fcntl.h>
+#include <unistd.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cerrno>
 #include <cstdio>
 #include <cstdlib>
@@ -311,6 +314,39 @@ void tns_parse_device(const char *h_bytes, uint64_t len, uint32_t &order, uint32
   nnz = nrec;
 }
 
+// Reads `len` bytes of `path` from offset `off` into dst with up to 16
+// threads, each taking 16 MiB pieces with pread: a file in the page cache
+// then arrives at memory-copy speed rather than at one thread's.
+static void read_parallel(const char *path, uint64_t off, uint64_t len, char *dst) {
+  if (!len) return;
+  const int fd = ::open(path, O_RDONLY);
+  if (fd < 0) fail(SYMPROP_ERR_INVALID, "cannot open %s", path);
+  const uint64_t piece = 16ull << 20, npieces = (len + piece - 1) / piece;
+  const unsigned nth =
+      (unsigned)std::min<uint64_t>(npieces, std::max(1u, std::min(16u, std::thread::hardware_concurrency())));
+  std::atomic<uint64_t> next{0};
+  std::atomic<bool> bad{false};
+  auto work = [&] {
+    for (uint64_t k; !bad && (k = next++) < npieces;) {
+      const uint64_t a = k * piece, n = std::min(piece, len - a);
+      for (uint64_t done = 0; done < n;) {
+        const ssize_t r = ::pread(fd, dst + a + done, n - done, (off_t)(off + a + done));
+        if (r <= 0) {
+          bad = true;
+          break;
+        }
+        done += (uint64_t)r;
+      }
+    }
+  };
+  std::vector<std::thread> pool;
+  for (unsigned i = 1; i < nth; ++i) pool.emplace_back(work);
+  work();
+  for (auto &th : pool) th.join();
+  ::close(fd);
+  if (bad) fail(SYMPROP_ERR_INVALID, "short read of %s", path);
+}
+
 }  // namespace spb
 
 using namespace spb;
@@ -338,9 +374,9 @@ int symprop_tensor_load_tns(const char *path, symprop_tensor **out) {
       fail(SYMPROP_ERR_OOM, "pinned host buffer of %ld bytes", sz);
     }
     std::unique_ptr<char, void (*)(char *)> hold(buf, [](char *p) { if (p) cudaFreeHost(p); });
-    const size_t got = sz > 0 ? std::fread(buf, 1, (size_t)sz, f) : 0;
     std::fclose(f);
-    if (got != (size_t)std::max(sz, 0L)) fail(SYMPROP_ERR_INVALID, "short read of %s", path);
+    const size_t got = (size_t)std::max(sz, 0L);
+    read_parallel(path, 0, got, buf);
     uint32_t order = 0, dim = 0;
     uint64_t nnz = 0;
     DBuf<uint32_t> inds;
@@ -393,8 +429,7 @@ int symprop_tensor_load_spt(const char *path, symprop_tensor **out) {
       fail(SYMPROP_ERR_OOM, "pinned host buffer of %llu bytes", (unsigned long long)(ibytes + vbytes));
     }
     std::unique_ptr<char, void (*)(char *)> hold(buf, [](char *p) { if (p) cudaFreeHost(p); });
-    if (ibytes + vbytes && std::fread(buf, 1, ibytes + vbytes, f) != ibytes + vbytes)
-      fail(SYMPROP_ERR_INVALID, "short read of %s", path);
+    read_parallel(path, sizeof head, ibytes + vbytes, buf);
     DBuf<uint32_t> inds(nnz * order);
     DBuf<double> vals(nnz);
     if (nnz) {
