@@ -104,9 +104,13 @@ __device__ __forceinline__ void ffma2(T &d0, T &d1, T a0, T a1, T b0, T b1) {
 }
 
 // CTAs per SM the register budget is sized for (accumulators: NTL x 16
-// values per lane)
-template <typename T, int NTL> __host__ __device__ constexpr int min_blocks() {
-  return sizeof(T) == 8 ? (NTL == 1 ? 4 : NTL <= 3 ? 3 : 2) : (NTL <= 3 ? 4 : 3);
+// values per lane).  FP64 with 2-3 tiles per thread takes 3 CTAs (168
+// registers) up to order 5; from order 6 on (L >= 5) the parents of the
+// last level need more, and 2 CTAs without spills beat 3 with them (order
+// 6, R = 10, 200k tuples: 9.8 against 12.6 ms; orders 4 and 5 are 15% and
+// 7% slower with 2).
+template <typename T, int NTL, int L> __host__ __device__ constexpr int min_blocks() {
+  return sizeof(T) == 8 ? (NTL == 1 ? 4 : (NTL <= 3 && L < 5) ? 3 : 2) : (NTL <= 3 ? 4 : 3);
 }
 
 // Team kernel: owners advanced per pipeline step (two halve the barriers;
@@ -388,7 +392,7 @@ __device__ __forceinline__ void write_tiles(const WarpParams &p, const Chunk &ch
 // Independent warps: one warp per work item, all of the row's tiles in its
 // lanes' registers; no barrier in the owner loop.
 template <int L, int NTL, typename T>
-__global__ void __launch_bounds__(kThreads, (min_blocks<T, NTL>())) s3ttmc_warp_kernel(const WarpParams p) {
+__global__ void __launch_bounds__(kThreads, (min_blocks<T, NTL, L>())) s3ttmc_warp_kernel(const WarpParams p) {
   constexpr bool kExact = sizeof(T) == 8;
   constexpr int kP = stage_per_lane<L>();
   extern __shared__ __align__(16) unsigned char smem[];
@@ -521,7 +525,7 @@ __global__ void __launch_bounds__(kThreads, (min_blocks<T, NTL>())) s3ttmc_warp_
 // step s, level d built at step s+d-1, its tiles added at step s+L-2, each
 // owner in its own buffer (L-1 buffers).
 template <int L, int NTL, typename T>
-__global__ void __launch_bounds__(kThreads, (min_blocks<T, NTL>())) s3ttmc_team_kernel(const WarpParams p) {
+__global__ void __launch_bounds__(kThreads, (min_blocks<T, NTL, L>())) s3ttmc_team_kernel(const WarpParams p) {
   constexpr bool kExact = sizeof(T) == 8;
   constexpr int kD = L - 1;                // pipeline depth (steps)
   constexpr int kOps = team_owners_per_step(L);  // owners per step (one barrier each)
