@@ -104,13 +104,14 @@ __device__ __forceinline__ void ffma2(T &d0, T &d1, T a0, T a1, T b0, T b1) {
 }
 
 // CTAs per SM the register budget is sized for (accumulators: NTL x 16
-// values per lane).  FP64 with 2-3 tiles per thread takes 3 CTAs (168
-// registers) up to order 5; from order 6 on (L >= 5) the parents of the
-// last level need more, and 2 CTAs without spills beat 3 with them (order
-// 6, R = 10, 200k tuples: 9.8 against 12.6 ms; orders 4 and 5 are 15% and
-// 7% slower with 2).
+// values per lane).  With up to 3 tiles per thread FP64 takes 3 CTAs (168
+// registers) and FP32 4 (128) up to order 5; from order 6 on (L >= 5) the
+// parents of the last level need more registers, and one CTA fewer without
+// spills beats the spills (order 6, R = 10, 200k tuples: FP64 9.8 against
+// 12.6 ms, FP32 7.2 against 7.5; orders 4 and 5 in FP64 are 15% and 7%
+// slower with 2 CTAs).
 template <typename T, int NTL, int L> __host__ __device__ constexpr int min_blocks() {
-  return sizeof(T) == 8 ? (NTL == 1 ? 4 : (NTL <= 3 && L < 5) ? 3 : 2) : (NTL <= 3 ? 4 : 3);
+  return sizeof(T) == 8 ? (NTL == 1 ? 4 : (NTL <= 3 && L < 5) ? 3 : 2) : ((NTL <= 3 && L < 5) ? 4 : 3);
 }
 
 // Team kernel: owners advanced per pipeline step (two halve the barriers;
