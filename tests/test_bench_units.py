@@ -35,3 +35,15 @@ def test_order6_units():
 
 def test_packed_sizes():
     assert [bench.msize(r, L) for r, L in [(16, 3), (16, 4), (10, 5), (8, 4)]] == [816, 3876, 2002, 330]
+
+
+def test_numa_binding_leaves_the_process_alone_without_a_gpu():
+    """bench.bind_near_gpu moves the process to the GPU's NUMA node through
+    NVML; with no GPU (or no NVML) it changes nothing and says so."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is visible: the binding would apply")
+    before = os.sched_getaffinity(0)
+    note, prev = bench.bind_near_gpu(0)
+    assert note.startswith("unchanged") and prev == before
+    assert os.sched_getaffinity(0) == before
