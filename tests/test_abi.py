@@ -44,6 +44,29 @@ def test_headers_compile_as_c_and_cpp(tmp_path):
                     str(tmp_path / "t.o")], check=True)
     cpp = tmp_path / "t.cpp"
     cpp.write_text('#include "symtucker.hpp"\nint main(){symprop::Config c; return (int)c.rank - 2;}\n')
+    # the reference's API and this library's additions compile as a caller writes them
+    api = tmp_path / "api.cpp"
+    api.write_text('''#include "symtucker.hpp"
+using namespace symprop;
+int use(const char *path) {
+  SpSymtensor X = SpSymtensor::load(path);
+  X.save_spt("x.spt");
+  std::vector<real_t> U(X.dim() * 4), Y(X.dim() * symtens_size(4, X.order() - 1)), C(4 * 4);
+  X.S3TTMc(Y, U, 4, true);
+  matrix::gemmtn(C, U, U, X.dim(), 4, 4);
+  matrix::qr(U, X.dim(), 4);
+  std::vector<real_t> coeff = symtens_coeff(4, X.order() - 1), F((size_t)X.dim() * X.dim());
+  matrix::symgemm(F, Y, Y, coeff, X.dim(), X.dim());
+  Config c;
+  c.rank = 4;
+  SymTuckerDecomp d = X.TuckerHOOI(c);
+  d.print(std::cout);
+  FunctionTimer::printTimes();
+  return (int)X.size();
+}
+''')
+    subprocess.run(["/usr/bin/g++", "-std=c++20", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"), "-c",
+                    str(api), "-o", str(tmp_path / "api.o")], check=True)
     subprocess.run(["/usr/bin/g++", "-std=c++20", "-I", os.path.join(ROOT, "include"), "-c",
                     str(cpp), "-o", str(tmp_path / "t2.o")], check=True)
 
