@@ -13,7 +13,7 @@
 //
 // Kernel: one CTA per 128 x 128 upper-triangular tile of G, 128 threads.
 //   warp 0 lane 0: TMA producer (cp.async.bulk.tensor, 128B swizzle,
-//                  6-stage mbarrier ring, no multicast)
+//                  6-stage mbarrier ring; each CTA loads its own tiles)
 //   warp 1 lane 0: MMA issuer (tcgen05.mma.cta_group::1.kind::f16, M=N=128,
 //                  K=16 per instruction, accumulator in 128 TMEM columns;
 //                  tcgen05.commit releases each smem stage)
