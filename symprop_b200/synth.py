@@ -29,16 +29,43 @@ __all__ = [
 
 def _unique_rows(t: np.ndarray) -> np.ndarray:
     """Unique rows of a sorted-within-row uint32 matrix, first occurrence kept,
-    original order preserved."""
+    original order preserved.  Each row is packed into as few 63-bit keys as
+    hold it (most significant first), the rows are ordered by stable
+    multi-threaded sorts of those keys, least significant key first, and the
+    first row of every run of equal keys is kept."""
+    import torch
     if t.shape[0] == 0:
         return t
-    order = np.lexsort(t.T[::-1])
-    s = t[order]
-    keep = np.ones(s.shape[0], dtype=bool)
-    keep[1:] = np.any(s[1:] != s[:-1], axis=1)
-    first = order[keep]
-    first.sort()
-    return t[first]
+    k, order = t.shape
+    bits = max(1, int(t.max()).bit_length())
+    per = 63 // bits
+    keys = []
+    for s0 in range(0, order, per):
+        w = np.zeros(k, dtype=np.int64)
+        for j in range(s0, min(order, s0 + per)):
+            w = (w << bits) | t[:, j].astype(np.int64)
+        keys.append(torch.from_numpy(w))
+    perm = torch.arange(k)
+    for w in reversed(keys):
+        _, idx = torch.sort(w[perm], stable=True)
+        perm = perm[idx]
+    new_run = torch.zeros(k - 1, dtype=torch.bool)
+    for w in keys:
+        ws = w[perm]
+        new_run |= ws[1:] != ws[:-1]
+    keep = torch.ones(k, dtype=torch.bool)
+    keep[1:] = new_run
+    first, _ = torch.sort(perm[keep])
+    return t[first.numpy()]
+
+
+def _inverse_cdf(cdf: np.ndarray, u: np.ndarray) -> np.ndarray:
+    """np.searchsorted(cdf, u, side="right"), computed with torch's
+    multi-threaded search (the same comparisons, so the same indices)."""
+    import torch
+    r = torch.searchsorted(torch.from_numpy(np.ascontiguousarray(cdf)),
+                           torch.from_numpy(np.ascontiguousarray(u)).reshape(-1), right=True)
+    return r.numpy().reshape(u.shape)
 
 
 def _draw_unique(draw, nnz: int, order: int, rng) -> np.ndarray:
@@ -66,7 +93,7 @@ def zipf_tuples(order: int, n: int, nnz: int, s: float, seed: int) -> np.ndarray
     perm = rng.permutation(n).astype(np.uint32)
 
     def draw(k):
-        r = np.searchsorted(cdf, rng.random((k, order)), side="right")
+        r = _inverse_cdf(cdf, rng.random((k, order)))
         return perm[np.minimum(r, n - 1)]
 
     return _draw_unique(draw, nnz, order, rng)
@@ -108,14 +135,14 @@ def powerlaw_communities(order: int, n: int, nnz: int, gamma: float,
         t = np.empty((k, order), dtype=np.int64)
         inside = rng.random(k) < frac_in
         u = rng.random((k, order))
-        g = np.minimum(np.searchsorted(global_cdf, u, side="right"), n - 1)
+        g = np.minimum(_inverse_cdf(global_cdf, u), n - 1)
         t[:] = g
         cs = rng.integers(0, communities, size=k)
         for c in range(communities):
             sel = inside & (cs == c)
             if not np.any(sel):
                 continue
-            idx = np.minimum(np.searchsorted(cdfs[c], u[sel], side="right"),
+            idx = np.minimum(_inverse_cdf(cdfs[c], u[sel]),
                              len(members[c]) - 1)
             t[sel] = members[c][idx]
         return t.astype(np.uint32)
@@ -144,7 +171,7 @@ def community_zipf(order: int, n: int, nnz: int, communities: int, s: float, see
     perm = rng.permutation(n)
 
     def draw(k):
-        t = perm[np.minimum(np.searchsorted(call, rng.random((k, order)), side="right"), n - 1)].astype(np.int64)
+        t = perm[np.minimum(_inverse_cdf(call, rng.random((k, order))), n - 1)].astype(np.int64)
         inside = rng.random(k) < frac_in
         cs = rng.integers(0, communities, size=k)
         for c in range(communities):
@@ -152,7 +179,7 @@ def community_zipf(order: int, n: int, nnz: int, communities: int, s: float, see
             cnt = int(sel.sum())
             if not cnt:
                 continue
-            idx = np.minimum(np.searchsorted(cdfs[c], rng.random((cnt, order)), side="right"),
+            idx = np.minimum(_inverse_cdf(cdfs[c], rng.random((cnt, order))),
                              len(members[c]) - 1)
             t[sel] = members[c][idx]
         return t.astype(np.uint32)
