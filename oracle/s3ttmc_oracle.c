@@ -23,6 +23,7 @@
  *   S3TTMc (opt5 math) ............ src/compressed_dtree.cpp:421-518,
  *                                   src/sparse/spsymtensor.cpp:30-110
  *   calc_norm ..................... src/sparse/spsymtensor.cpp:114-138
+ *   S3TTMc on listed rows ......... the same owners as S3TTMc, other rows skipped
  */
 #include <math.h>
 #include <stdint.h>
@@ -130,7 +131,7 @@ void orc_symtens_coeff(uint32_t dim, int N, double *coeff) {
 }
 
 /* dst (order L) += SymOuterProd(src (order L-1), row) */
-void orc_sym_outer_prod(double *dst, const double *src, const double *row,
+void orc_sym_outer_prod(double *restrict dst, const double *restrict src, const double *restrict row,
                         uint32_t dim, int L) {
   if (L == 1) {
     for (uint32_t c = 0; c < dim; c++) dst[c] += src[0] * row[c];
@@ -240,6 +241,106 @@ int orc_s3ttmc(uint32_t order, uint32_t dim, uint64_t nnz, const uint32_t *inds,
     free(row);
   }
   return 0;
+}
+
+/* K(S) as leaf_tensor computes it, with the level tensors in a caller-owned
+ * workspace (one block of orc_leaf_ws_size(R, L) doubles) instead of one
+ * allocation per position subset. */
+static uint64_t orc_leaf_ws_size(uint32_t R, int L) {
+  uint64_t tot = 0;
+  for (int mask = 1; mask < (1 << L); mask++)
+    tot += orc_symtens_size(R, (uint64_t)__builtin_popcount((unsigned)mask));
+  return tot;
+}
+
+static void leaf_tensor_ws(const uint32_t *S, int L, const double *U, uint32_t R,
+                           double *ws, double *out) {
+  double *K[1 << 12]; /* L <= 12 (checked by the caller) */
+  double *next = ws;
+  for (int mask = 1; mask < (1 << L); mask++) {
+    int pc = __builtin_popcount((unsigned)mask);
+    uint64_t sz = orc_symtens_size(R, (uint64_t)pc);
+    K[mask] = next;
+    next += sz;
+    if (pc == 1) {
+      memcpy(K[mask], U + (uint64_t)S[__builtin_ctz((unsigned)mask)] * R, sizeof(double) * R);
+      continue;
+    }
+    memset(K[mask], 0, sizeof(double) * sz);
+    for (int k = 0; k < L; k++) {
+      if (!(mask & (1 << k))) continue;
+      orc_sym_outer_prod(K[mask], K[mask & ~(1 << k)], U + (uint64_t)S[k] * R, R, pc);
+    }
+  }
+  memcpy(out, K[(1 << L) - 1], sizeof(double) * orc_symtens_size(R, (uint64_t)L));
+}
+
+/* The packed Y of orc_s3ttmc restricted to the listed rows: Yrows[k] is
+ * row rows[k] (0-based ids, distinct), nrows x C(R+N-2, N-1).  The owners
+ * are those of orc_s3ttmc (every tuple, every removed position j, Y[t_j] +=
+ * coef K(S)), and the owners of unlisted rows are skipped, so checking a few
+ * rows of a large tensor costs only their owners.  The owners are divided
+ * among OpenMP threads, each summing into its own copy of the listed rows;
+ * the copies are added at the end. */
+int orc_s3ttmc_rows(uint32_t order, uint32_t dim, uint64_t nnz, const uint32_t *inds,
+                    const double *vals, uint32_t R, const double *U, uint64_t nrows,
+                    const uint32_t *rows, double *Yrows) {
+  int N = (int)order, L = N - 1;
+  if (N < 2 || N > ORC_MAXL || L > 12) return -1;
+  uint64_t m = orc_symtens_size(R, (uint64_t)L);
+  memset(Yrows, 0, sizeof(double) * m * nrows);
+  if (N == 2 || nrows == 0) return 0; /* reference: empty level loop, Y stays 0 */
+  int64_t *slot = (int64_t *)malloc(sizeof(int64_t) * dim);
+  if (!slot) return -2;
+  for (uint32_t i = 0; i < dim; i++) slot[i] = -1;
+  for (uint64_t k = 0; k < nrows; k++) {
+    if (rows[k] >= dim || slot[rows[k]] >= 0) {
+      free(slot);
+      return -1;
+    }
+    slot[rows[k]] = (int64_t)k;
+  }
+  uint64_t wsz = orc_leaf_ws_size(R, L);
+  int fail = 0;
+#pragma omp parallel
+  {
+    double *mine = (double *)calloc(m * nrows, sizeof(double));
+    double *ws = (double *)malloc(sizeof(double) * wsz);
+    double *Kbuf = (double *)malloc(sizeof(double) * m);
+    if (!mine || !ws || !Kbuf) {
+#pragma omp atomic write
+      fail = 1;
+    } else {
+      uint32_t t[ORC_MAXL], S[ORC_MAXL];
+#pragma omp for schedule(dynamic, 256)
+      for (uint64_t i = 0; i < nnz; i++) {
+        int any = 0;
+        for (int j = 0; j < N; j++) {
+          t[j] = inds[i * N + j] - 1;
+          any |= slot[t[j]] >= 0;
+        }
+        if (!any) continue;
+        double coef = vals[i] * (double)orc_multinomial_sorted(t, N) / (double)FACT[N];
+        for (int j = N - 1; j >= 0; j--) {
+          int64_t k = slot[t[j]];
+          if (k < 0) continue;
+          int c = 0;
+          for (int q = 0; q < N; q++)
+            if (q != j) S[c++] = t[q];
+          leaf_tensor_ws(S, L, U, R, ws, Kbuf);
+          double *y = mine + (uint64_t)k * m;
+          for (uint64_t q = 0; q < m; q++) y[q] += coef * Kbuf[q];
+        }
+      }
+#pragma omp critical
+      for (uint64_t q = 0; q < m * nrows; q++) Yrows[q] += mine[q];
+    }
+    free(mine);
+    free(ws);
+    free(Kbuf);
+  }
+  free(slot);
+  return fail ? -2 : 0;
 }
 
 double orc_norm(uint32_t order, uint64_t nnz, const uint32_t *inds,

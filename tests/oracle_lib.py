@@ -48,6 +48,9 @@ def olib():
         L.orc_symtens_coeff.argtypes = [ctypes.c_uint32, ctypes.c_int, _P]
         L.orc_sym_outer_prod.argtypes = [_P, _P, _P, ctypes.c_uint32, ctypes.c_int]
         L.orc_unpack.argtypes = [_P, ctypes.c_uint32, ctypes.c_int, _P]
+        L.orc_s3ttmc_rows.restype = ctypes.c_int
+        L.orc_s3ttmc_rows.argtypes = [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64, _P, _P,
+                                      ctypes.c_uint32, _P, ctypes.c_uint64, _P, _P]
         L.orc_multinomial_sorted.restype = ctypes.c_uint64
         L.orc_multinomial_sorted.argtypes = [_P, ctypes.c_int]
         _lib = L
@@ -67,6 +70,20 @@ def s3ttmc(order, dim, inds, vals, U, R, packed=True):
     Y = np.zeros((dim, cols))
     st = L.orc_s3ttmc(order, dim, vals.shape[0], p(inds), p(vals), R, p(U), int(packed), p(Y))
     assert st == 0
+    return Y
+
+
+def s3ttmc_rows(order, dim, inds, vals, U, R, rows):
+    """Packed Y of the oracle on the listed rows only (0-based, distinct):
+    len(rows) x C(R+N-2, N-1)."""
+    L = olib()
+    inds = np.ascontiguousarray(inds, np.uint32)
+    vals = np.ascontiguousarray(vals, np.float64)
+    U = np.ascontiguousarray(U, np.float64)
+    rows = np.ascontiguousarray(rows, np.uint32)
+    Y = np.zeros((rows.shape[0], L.orc_symtens_size(R, order - 1)))
+    st = L.orc_s3ttmc_rows(order, dim, vals.shape[0], p(inds), p(vals), R, p(U), rows.shape[0], p(rows), p(Y))
+    assert st == 0, st
     return Y
 
 
