@@ -99,6 +99,9 @@ def lib():
         "symprop_gram_device": (_I, [_P, _U64, _U32, _P, _P, _I, _P]),
         "symprop_s3ttmc_schedule": (_I, [_I]),
         "symprop_gram_device_noalloc": (_I, [_P, _U64, _U32, _P, _P, _P]),
+        "symprop_symsyrk_device": (_I, [_P, _P, _P, _U64, _U64, _P]),
+        "symprop_symgemm_device": (_I, [_P, _P, _P, _P, _U64, _U64, _U64, _P]),
+        "symprop_debug_set_tc_wait_ns": (_I, [_U64]),
         "symprop_tensor_load_tns": (_I, [ctypes.c_char_p, ctypes.POINTER(_P)]),
         "symprop_tensor_copy_nonzeros": (_I, [_P, _P, _P]),
         "symprop_tensor_load_spt": (_I, [ctypes.c_char_p, ctypes.POINTER(_P)]),
@@ -130,6 +133,7 @@ def exported_symbols() -> list[str]:
         "symprop_tensor_load_tns", "symprop_tensor_copy_nonzeros", "symprop_tensor_load_spt",
         "symprop_tensor_save_spt",
         "symprop_gemmtn", "symprop_symgemm", "symprop_symsyrk", "symprop_qr", "symprop_syevd", "symprop_leftsvd",
+        "symprop_symsyrk_device", "symprop_symgemm_device", "symprop_debug_set_tc_wait_ns",
     ]
 
 
@@ -154,6 +158,20 @@ def gram_device(dY_ptr: int, n: int, m: int, dscale_ptr: int, dG_ptr: int, preci
     """G = (Y diag(scale))^T (Y diag(scale)) on the device (FP64 CUDA cores or
     FP32 input on tcgen05 tensor cores with split-BF16 operands)."""
     _check(lib().symprop_gram_device(_P(dY_ptr), n, m, _P(dscale_ptr), _P(dG_ptr), precision, _P(stream)))
+
+
+def symsyrk_device(dA_ptr: int, dscale_ptr: int, dC_ptr: int, ncoeff: int, I1: int, stream: int = 0) -> None:
+    """C (I1 x I1, FP64) = (A diag(scale)) (A diag(scale))^T for an FP32 device
+    A (I1 x ncoeff) and FP32 scale, on the tensor cores (split-BF16)."""
+    _check(lib().symprop_symsyrk_device(_P(dA_ptr), _P(dscale_ptr), _P(dC_ptr), ncoeff, I1, _P(stream)))
+
+
+def symgemm_device(dA_ptr: int, dB_ptr: int, dscale_ptr: int, dC_ptr: int, ncoeff: int, I1: int, I2: int,
+                   stream: int = 0) -> None:
+    """C (I1 x I2, FP64) = (A diag(scale)) (B diag(scale))^T for an FP32 device
+    A (I1 x ncoeff), FP64 B (I2 x ncoeff) and FP64 scale, on the tensor cores."""
+    _check(lib().symprop_symgemm_device(_P(dA_ptr), _P(dB_ptr), _P(dscale_ptr), _P(dC_ptr), ncoeff, I1, I2,
+                                        _P(stream)))
 
 
 class matrix:

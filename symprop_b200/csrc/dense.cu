@@ -530,6 +530,55 @@ struct Scratch {
   template <class T> T *as() { return reinterpret_cast<T *>(p); }
 };
 
+// Partial core products P[chunk][q][j] = sum_{i in chunk} U[i][q0 + q] Y[i][j]
+// over FP32 Y (n x m, read once, coalesced along j) and FP64 U (n x r): one
+// thread per column j, kCoreRB FP64 accumulators, the U rows of the chunk
+// staged in shared memory 64 at a time (every thread reads the same entry).
+constexpr int kCoreRB = 16, kCoreRows = 64;
+__global__ void __launch_bounds__(128) core_partial_kernel(const double *__restrict__ U,
+                                                           const float *__restrict__ Y, int n, int m,
+                                                           int r, int q0, int rows_per_chunk,
+                                                           double *__restrict__ P) {
+  __shared__ double Us[kCoreRows][kCoreRB];
+  const int col = blockIdx.x * 128 + threadIdx.x;
+  const int i0 = blockIdx.y * rows_per_chunk, i1 = min(n, i0 + rows_per_chunk);
+  double acc[kCoreRB];
+#pragma unroll
+  for (int q = 0; q < kCoreRB; ++q) acc[q] = 0.0;
+  for (int ib = i0; ib < i1; ib += kCoreRows) {
+    for (int t = threadIdx.x; t < kCoreRows * kCoreRB; t += 128) {
+      const int ii = t / kCoreRB, q = t % kCoreRB;
+      Us[ii][q] = (ib + ii < i1 && q0 + q < r) ? U[(size_t)(ib + ii) * r + q0 + q] : 0.0;
+    }
+    __syncthreads();
+    const int cnt = min(kCoreRows, i1 - ib);
+    if (col < m) {
+      for (int ii = 0; ii < cnt; ++ii) {
+        const double y = (double)Y[(size_t)(ib + ii) * m + col];
+#pragma unroll
+        for (int q = 0; q < kCoreRB; ++q) acc[q] = fma(Us[ii][q], y, acc[q]);
+      }
+    }
+    __syncthreads();
+  }
+  if (col < m) {
+#pragma unroll
+    for (int q = 0; q < kCoreRB; ++q) P[((size_t)blockIdx.y * kCoreRB + q) * m + col] = acc[q];
+  }
+}
+
+// core[q0 + q][j] = sum over chunks (in chunk order) of P[chunk][q][j]
+__global__ void core_reduce_kernel(const double *__restrict__ P, int chunks, int m, int r, int q0,
+                                   double *__restrict__ core) {
+  const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (size_t)kCoreRB * m) return;
+  const int q = (int)(idx / m), j = (int)(idx % m);
+  if (q0 + q >= r) return;
+  double s = 0.0;
+  for (int c = 0; c < chunks; ++c) s += P[((size_t)c * kCoreRB + q) * m + j];
+  core[(size_t)(q0 + q) * m + j] = s;
+}
+
 }  // namespace
 
 // ------------------------------------------------------------ public API
@@ -577,6 +626,28 @@ template void gemm<double>(cudaStream_t, int, int, int, double, const double *, 
                            const double *, int, bool, double, double *, int, const double *, bool);
 template void gemm<float>(cudaStream_t, int, int, int, float, const float *, int, bool,
                           const float *, int, bool, float, float *, int, const float *, bool);
+
+void core_from_f32(cudaStream_t st, const double *U, const float *Y, int n, int m, int r, double *core) {
+  if (r <= 0 || m <= 0) return;
+  if (n <= 0) {
+    SPB_CUDA(cudaMemsetAsync(core, 0, sizeof(double) * (size_t)r * m, st));
+    return;
+  }
+  const int colblocks = (int)cdiv(m, 128);
+  // about 8 CTAs per SM in all, each chunk a multiple of the staging depth
+  int chunks = std::max(1, std::min((int)cdiv(1184, colblocks), (int)cdiv(n, 4 * kCoreRows)));
+  const int rows_per_chunk = (int)(cdiv(cdiv(n, chunks), kCoreRows) * kCoreRows);
+  chunks = (int)cdiv(n, rows_per_chunk);
+  Scratch part(sizeof(double) * (size_t)chunks * kCoreRB * m, st);
+  for (int q0 = 0; q0 < r; q0 += kCoreRB) {
+    core_partial_kernel<<<dim3(colblocks, chunks), 128, 0, st>>>(U, Y, n, m, r, q0, rows_per_chunk,
+                                                                 part.as<double>());
+    SPB_LAUNCH_CHECK();
+    core_reduce_kernel<<<cdiv((long long)kCoreRB * m, 256), 256, 0, st>>>(part.as<double>(), chunks, m, r, q0,
+                                                                          core);
+    SPB_LAUNCH_CHECK();
+  }
+}
 
 template <typename T>
 void weighted_sq(cudaStream_t st, const T *X, const T *Y, const double *w, int rows, int cols,

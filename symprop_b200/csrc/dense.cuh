@@ -21,6 +21,11 @@ void gemm(cudaStream_t st, int M, int N, int K, T alpha, const T *A, int lda, bo
           const T *B, int ldb, bool transB, T beta, T *C, int ldc, const T *kscale = nullptr,
           bool sym_upper = false);
 
+// core (r x m, FP64) = U^T Y for FP64 U (n x r) and FP32 Y (n x m), both
+// row-major: Y is read once and widened in registers, FP64 accumulation,
+// deterministic (fixed row chunks summed in order).
+void core_from_f32(cudaStream_t st, const double *U, const float *Y, int n, int m, int r, double *core);
+
 // sum_{i<rows, q<cols} w[q] * (X[i,q] - (Y ? Y[i,q] : 0))^2 and sum w X^2 (FP64 out, deterministic)
 template <typename T>
 void weighted_sq(cudaStream_t st, const T *X, const T *Y, const double *w, int rows, int cols,

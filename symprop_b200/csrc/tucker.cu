@@ -173,18 +173,27 @@ int run_tucker(TensorState &t, const symprop_config &c, int alg, symprop_result 
 
   const bool gram_nn = n <= m;  // n x n form (AltHOOI's symsyrk) vs m x m Gram
   const int s = gram_nn ? n : m;
-  DBuf<double> Y((size_t)n * m);
-  DBuf<float> Y32(mixed ? (size_t)n * m : 0), U32(mixed ? (size_t)n * r : 0);
-  DBuf<float> S32(mixed ? (size_t)s * s : 0), V32(mixed ? (size_t)s * r : 0),
-      core32(mixed ? (size_t)r * m : 0), W32(mixed ? (size_t)n * r : 0), sD32(mixed ? m : 0),
-      D32(mixed ? m : 0);
-  if (mixed) {
-    dense::convert<double, float>(st, dsD.p, sD32.p, m);
-    dense::convert<double, float>(st, dD.p, D32.p, m);
-  }
-  DBuf<char> gram_ws(mixed && !gram_nn ? gram::workspace_bytes(n, m) : 0);
+  // FP64 Y: allocated when an FP64 S3TTMc first runs (the mixed driver may
+  // finish in FP64)
+  DBuf<double> Y(mixed ? 0 : (size_t)n * m);
+  // mixed: FP32 Y and U, the split-BF16 operand Z = Y D^1/2 ~ H + L and the
+  // tensor-core products' scratch
+  DBuf<float> Y32(mixed ? (size_t)n * m : 0), U32(mixed ? (size_t)n * r : 0), sD32(mixed ? m : 0);
+  DBuf<char> split_ws(mixed ? gram::split_bytes(n, m) : 0);
+  DBuf<char> gram_scr(mixed && alg != SYMPROP_HOQRI
+                          ? (gram_nn ? gram::gram_rows_scratch_bytes(n, m) : gram::gram_cols_scratch_bytes(n, m))
+                          : 0);
+  DBuf<char> times_scr(mixed ? gram::times_scratch_bytes(n, m) : 0);
+  const gram::Split Z = mixed ? gram::split_view(split_ws.p, n, m) : gram::Split{};
+  if (mixed) dense::convert<double, float>(st, dsD.p, sD32.p, m);
   DBuf<int> gram_err(1);
   SPB_CUDA(cudaMemsetAsync(gram_err.p, 0, sizeof(int), st));
+  // W (n x r) = Z P^T on the tensor cores, 16 columns of W per product
+  auto tc_times = [&](const double *P, size_t sq, size_t sk, const double *colscale, double *W) {
+    for (int q0 = 0; q0 < r; q0 += gram::kPanelRows)
+      gram::times(st, Z, P + q0 * sq, std::min(gram::kPanelRows, r - q0), sq, sk, colscale, W + q0,
+                  (size_t)r, times_scr.p, gram_err.p);
+  };
   DBuf<double> S((size_t)s * s), V((size_t)s * r), Vwarm((size_t)s * r);
   DBuf<double> core((size_t)r * m), core_prev((size_t)r * m), red(2);
   SPB_CUDA(cudaMemsetAsync(core_prev.p, 0, sizeof(double) * r * m, st));
@@ -232,9 +241,11 @@ int run_tucker(TensorState &t, const symprop_config &c, int alg, symprop_result 
       dense::convert<double, float>(st, U.p, U32.p, (size_t)n * r);
       s3ttmc_run(t, U32.p, (uint32_t)r, true, Y32.p, SYMPROP_FP32, st);
     } else {
+      Y.ensure((size_t)n * m);
       s3ttmc_run(t, U.p, (uint32_t)r, true, Y.p, SYMPROP_FP64, st);
     }
     s3_ms += tphase.stop_ms();
+    const bool tc = mx;  // this iteration's dense products run on the tensor cores
 
     nvtxRangePushA("dense step");
     tphase.start();
@@ -243,8 +254,9 @@ int run_tucker(TensorState &t, const symprop_config &c, int alg, symprop_result 
       // leading r-dimensional left singular subspace of Y D^1/2
       if (gram_nn) {
         if (mx) {
-          dense::gemm<float>(st, n, n, m, 1.f, Y32.p, m, false, Y32.p, m, true, 0.f, S32.p, n, D32.p, true);
-          dense::convert<float, double>(st, S32.p, S.p, (size_t)n * n);
+          // tensor-core split-BF16 Gram of the rows of Y D^1/2 (FP32 accumulation)
+          gram::split(st, Y32.p, sD32.p, Z);
+          gram::gram_rows(st, Z, S.p, gram_scr.p, gram_err.p);
         } else {
           dense::gemm<double>(st, n, n, m, 1.0, Y.p, m, false, Y.p, m, true, 0.0, S.p, n, dD.p, true);
         }
@@ -254,8 +266,9 @@ int run_tucker(TensorState &t, const symprop_config &c, int alg, symprop_result 
         SPB_CUDA(cudaMemcpyAsync(U.p, V.p, sizeof(double) * n * r, cudaMemcpyDeviceToDevice, st));
       } else {
         if (mx) {
-          // tcgen05 split-BF16 Gram of Y D^1/2 (FP32 accumulation)
-          gram::gram_split_bf16(st, Y32.p, n, m, sD32.p, S.p, gram_ws.p, gram_err.p);
+          // tensor-core split-BF16 Gram of the columns of Y D^1/2
+          gram::split(st, Y32.p, sD32.p, Z);
+          gram::gram_cols(st, Z, S.p, gram_scr.p, gram_err.p);
         } else {
           dense::gemm<double>(st, m, m, n, 1.0, Y.p, m, true, Y.p, m, false, 0.0, S.p, m, nullptr, true);
           scale_sym_kernel<<<(unsigned)(((size_t)m * m + 255) / 256), 256, 0, st>>>(S.p, m, dsD.p);
@@ -265,9 +278,7 @@ int run_tucker(TensorState &t, const symprop_config &c, int alg, symprop_result 
                                 eig_tol, 60);
         if (e != SYMPROP_OK) warn_noconv(alg);
         if (mx) {
-          dense::convert<double, float>(st, V.p, V32.p, (size_t)m * r);
-          dense::gemm<float>(st, n, r, m, 1.f, Y32.p, m, false, V32.p, r, false, 0.f, W32.p, r, sD32.p);
-          dense::convert<float, double>(st, W32.p, U.p, (size_t)n * r);
+          tc_times(V.p, 1, (size_t)r, nullptr, U.p);  // U = Y D^1/2 V (P = V^T)
         } else {
           dense::gemm<double>(st, n, r, m, 1.0, Y.p, m, false, V.p, r, false, 0.0, U.p, r, dsD.p);
         }
@@ -276,9 +287,10 @@ int run_tucker(TensorState &t, const symprop_config &c, int alg, symprop_result 
       SPB_CUDA(cudaMemcpyAsync(Vwarm.p, V.p, sizeof(double) * (size_t)s * r, cudaMemcpyDeviceToDevice, st));
       have_warm = true;
       // core = U^T Y (r x m packed), FP64 in both modes: the objective and
-      // the convergence test read it (mixed: the FP32 Y widened first)
-      if (mx) dense::convert<float, double>(st, Y32.p, Y.p, (size_t)n * m);
-      dense::gemm<double>(st, r, m, n, 1.0, U.p, r, true, Y.p, m, false, 0.0, core.p, m);
+      // the convergence test read it (mixed: from the FP32 Y, widened in
+      // registers)
+      if (mx) dense::core_from_f32(st, U.p, Y32.p, n, m, r, core.p);
+      else dense::gemm<double>(st, r, m, n, 1.0, U.p, r, true, Y.p, m, false, 0.0, core.p, m);
       double h[2];
       if (alg == SYMPROP_HOOI) {
         // rel_residual(core_prev, core) on the unpacked cores
@@ -299,13 +311,12 @@ int run_tucker(TensorState &t, const symprop_config &c, int alg, symprop_result 
       cn2 = h[1];
     } else {  // HOQRI
       if (mx) {
-        // core in FP64 (objective), the update U = Y diag(D) core^T in FP32
-        // (symgemm, src/dense/matrixops.cpp:102-124)
-        dense::convert<float, double>(st, Y32.p, Y.p, (size_t)n * m);
-        dense::gemm<double>(st, r, m, n, 1.0, U.p, r, true, Y.p, m, false, 0.0, core.p, m);
-        dense::convert<double, float>(st, core.p, core32.p, (size_t)r * m);
-        dense::gemm<float>(st, n, r, m, 1.f, Y32.p, m, false, core32.p, m, true, 0.f, W32.p, r, D32.p);
-        dense::convert<float, double>(st, W32.p, U.p, (size_t)n * r);
+        // core in FP64 (objective) from the FP32 Y; the update
+        // U = Y diag(D) core^T (symgemm, src/dense/matrixops.cpp:102-124) as
+        // (Y D^1/2)(D^1/2 core^T) on the tensor cores
+        dense::core_from_f32(st, U.p, Y32.p, n, m, r, core.p);
+        gram::split(st, Y32.p, sD32.p, Z);
+        tc_times(core.p, (size_t)m, 1, dsD.p, U.p);
       } else {
         dense::gemm<double>(st, r, m, n, 1.0, U.p, r, true, Y.p, m, false, 0.0, core.p, m);
         dense::gemm<double>(st, n, r, m, 1.0, Y.p, m, false, core.p, m, true, 0.0, U.p, r, dD.p);
@@ -320,7 +331,7 @@ int run_tucker(TensorState &t, const symprop_config &c, int alg, symprop_result 
     }
     dense_ms += tphase.stop_ms();
     nvtxRangePop();
-    if (mx && !gram_nn) {
+    if (tc) {
       int herr = 0;
       SPB_CUDA(cudaMemcpy(&herr, gram_err.p, sizeof(int), cudaMemcpyDeviceToHost));
       if (herr) fail(SYMPROP_ERR_TIMEOUT, "tensor-core Gram: a bounded wait expired");

@@ -27,6 +27,37 @@ def test_device_out_of_memory_is_a_status(gpu):
     assert C.shape == (2, 4)
 
 
+def test_tensor_core_wait_expiry_is_a_status(gpu):
+    """The tcgen05 kernels bound every mbarrier wait.  The failure-injection
+    hook lowers the bound of the main-loop waits (TMA copies landing, MMAs
+    freeing a stage) to 1 ns, so waits that last longer than one tick of the
+    GPU's global timer expire.  The kernel must then drain the copies and
+    MMAs it issued, free its tensor memory and report SYMPROP_ERR_TIMEOUT,
+    and the next call, with the default bound, must give the right matrix."""
+    import torch
+    L = gpu.lib()
+    n, m = 50000, 330
+    g = torch.Generator(device="cpu").manual_seed(5)
+    Y = torch.randn(n, m, generator=g).cuda()
+    sd = (torch.rand(m, generator=g) + 0.5).cuda()
+    G = torch.empty(m, m, dtype=torch.float64, device="cuda")
+    P = ctypes.c_void_p
+    try:
+        assert L.symprop_debug_set_tc_wait_ns(1) == 0
+        st = L.symprop_gram_device(P(Y.data_ptr()), n, m, P(sd.data_ptr()), P(G.data_ptr()), gpu.FP32, None)
+        assert st == gpu.ERR_TIMEOUT, (st, L.symprop_last_error())
+        assert b"bounded wait" in L.symprop_last_error()
+    finally:
+        L.symprop_debug_set_tc_wait_ns(0)
+    st = L.symprop_gram_device(P(Y.data_ptr()), n, m, P(sd.data_ptr()), P(G.data_ptr()), gpu.FP32, None)
+    assert st == 0, L.symprop_last_error()
+    X = (Y * sd).double()
+    ref = X.T @ X
+    # FP32 accumulation on the tensor cores: one ulp per accumulator update
+    # (3 n / 16 updates) plus the split's 2^-17 per product
+    assert float((G - ref).norm() / ref.norm()) < 3 * n / 16 * 2.0 ** -24 + 1e-5
+
+
 def test_rank_above_dim_is_rejected(gpu):
     t = synth.zipf_tuples(3, 6, 10, 1.2, 1)
     X = gpu.SpSymtensor(6, 3, t, np.ones(t.shape[0]))
