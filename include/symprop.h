@@ -136,11 +136,12 @@ int symprop_s3ttmc(const symprop_tensor *t, const void *U, uint32_t R,
 int symprop_s3ttmc_device(const symprop_tensor *t, const void *dU, uint32_t R,
                           int packed, void *dY, int precision, void *stream);
 /* Selects the S3TTMc schedule for the whole process: 0 automatic (default:
- * warp-per-owner where the packed output fits one warp's registers, else
- * CTA register-tiled, else the per-owner rows kernel), 1 rows kernel,
- * 2 CTA register-tiled only, 3 warp-per-owner only (2 and 3 return
- * SYMPROP_ERR_SIZE on shapes they do not cover).  All compute the same Y;
- * tests use this to check each schedule against the oracle. */
+ * the pivot chain where it applies, else warp-per-owner where the packed
+ * output fits one warp's registers, else CTA register-tiled, else the
+ * per-owner rows kernel), 1 rows kernel, 2 CTA register-tiled only,
+ * 3 warp-per-owner only, 4 pivot chain only (2, 3 and 4 return
+ * SYMPROP_ERR_SIZE on shapes they do not cover).  All compute the same Y
+ * up to rounding; tests use this to check each schedule against the oracle. */
 int symprop_s3ttmc_schedule(int schedule);
 /* Number of kernel launches one symprop_s3ttmc_device call issues for
  * (R, packed); lets callers count their launches. */
@@ -178,12 +179,37 @@ int symprop_gram_device(const void *dY, uint64_t n, uint32_t m, const void *dsca
  * every GPU that loads the library until the process exits.  Inputs whose
  * workspace (about 4*m*n + 4*m*m bytes) exceeds it are rejected with
  * SYMPROP_ERR_SIZE.  The first call on each device looks the array up with
- * that device current; make that first call before any stream capture.
- * Every call reuses the same array, so calls that overlap on the GPU (other
- * streams, other host threads) race and must be serialised by the caller.
+ * that device current and keeps its address; make that first call before
+ * any stream capture, and do not use this entry point across a device reset.
+ * Every call reads its error flag back and synchronises `stream` before it
+ * returns.  Every call reuses the same array, so calls that overlap on the
+ * GPU (other streams, other host threads) race and must be serialised by
+ * the caller.  The result equals symprop_gram_device's (FP32) bit for bit.
  * This entry point has no counterpart in the reference. */
 int symprop_gram_device_noalloc(const float *dY, uint64_t n, uint32_t m, const float *dscale,
                                 double *dG, void *stream);
+
+/* Device forms of matrix::symsyrk and matrix::symgemm (src/dense/
+ * matrixops.cpp:126-146, :102-124) on the tcgen05 tensor cores, the dense
+ * products of mixed-precision HOOI and HOQRI.  A is an FP32 row-major
+ * I1 x ncoeff device matrix and scale a device vector of ncoeff column
+ * scales (the square roots of the reference's row_coeff); A diag(scale) is
+ * split into BF16 hi/lo parts and every product keeps three of the four
+ * hi/lo terms, with FP32 accumulation.  Both synchronise `stream`.
+ * symsyrk_device: C (I1 x I1, FP64, full symmetric) = (A diag(scale))
+ *   (A diag(scale))^T; dscale is float*.
+ * symgemm_device: C (I1 x I2, FP64, row-major) = (A diag(scale))
+ *   (B diag(scale))^T for an FP64 I2 x ncoeff B; dscale is double*. */
+int symprop_symsyrk_device(const float *dA, const float *dscale, double *dC, uint64_t ncoeff,
+                           uint64_t I1, void *stream);
+int symprop_symgemm_device(const float *dA, const double *dB, const double *dscale, double *dC,
+                           uint64_t ncoeff, uint64_t I1, uint64_t I2, void *stream);
+
+/* Failure injection for tests: bounds the tensor-core kernels' main-loop
+ * waits (TMA copies, MMA completion) at ns nanoseconds instead of 2 s; 0
+ * restores the default.  A wait that expires ends the call with
+ * SYMPROP_ERR_TIMEOUT after the kernel has drained what it issued. */
+int symprop_debug_set_tc_wait_ns(uint64_t ns);
 
 /* ------------------------------------------- matrix:: operations (host) */
 /* FP64 row-major matrices in host memory, computed on the current device:

@@ -192,7 +192,7 @@ int symprop_s3ttmc(const symprop_tensor *t, const void *U, uint32_t R, int packe
 
 int symprop_s3ttmc_schedule(int schedule) {
   return guard([&] {
-    require(schedule >= 0 && schedule <= 3, "schedule must be 0, 1, 2 or 3");
+    require(schedule >= 0 && schedule <= 4, "schedule must be 0, 1, 2, 3 or 4");
     set_s3ttmc_schedule(schedule);
   });
 }
@@ -201,6 +201,53 @@ int symprop_s3ttmc_launches(const symprop_tensor *t, uint32_t R, int packed, uin
   return guard([&] {
     require(t && launches, "null argument");
     *launches = s3ttmc_launch_count(t->s, R, packed != 0);
+  });
+}
+
+namespace {
+// *d_err of a tensor-core product, read after the stream drains
+void check_tc_err(cudaStream_t st, const int *d_err) {
+  int h = 0;
+  SPB_CUDA(cudaMemcpyAsync(&h, d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  SPB_CUDA(cudaStreamSynchronize(st));
+  if (h) fail(SYMPROP_ERR_TIMEOUT, "tensor-core product: a bounded wait expired");
+}
+}  // namespace
+
+int symprop_symsyrk_device(const float *dA, const float *dscale, double *dC, uint64_t ncoeff, uint64_t I1,
+                           void *stream) {
+  return guard([&] {
+    require(dA && dscale && dC, "null argument");
+    require(ncoeff > 0 && I1 > 0 && ncoeff < (1ull << 31) && I1 < (1ull << 31), "bad sizes");
+    cudaStream_t st = (cudaStream_t)stream;
+    DBuf<char> ws(gram::split_bytes((int)I1, (int)ncoeff)), scr(gram::gram_rows_scratch_bytes((int)I1, (int)ncoeff));
+    DBuf<int> err(1);
+    SPB_CUDA(cudaMemsetAsync(err.p, 0, sizeof(int), st));
+    const gram::Split z = gram::split_view(ws.p, (int)I1, (int)ncoeff);
+    gram::split(st, dA, dscale, z);
+    gram::gram_rows(st, z, dC, scr.p, err.p);
+    check_tc_err(st, err.p);
+  });
+}
+
+int symprop_symgemm_device(const float *dA, const double *dB, const double *dscale, double *dC,
+                           uint64_t ncoeff, uint64_t I1, uint64_t I2, void *stream) {
+  return guard([&] {
+    require(dA && dB && dscale && dC, "null argument");
+    require(ncoeff > 0 && I1 > 0 && I2 > 0 && ncoeff < (1ull << 31) && I1 < (1ull << 31) && I2 < (1ull << 20),
+            "bad sizes");
+    cudaStream_t st = (cudaStream_t)stream;
+    DBuf<char> ws(gram::split_bytes((int)I1, (int)ncoeff)), scr(gram::times_scratch_bytes((int)I1, (int)ncoeff));
+    DBuf<float> sc((size_t)ncoeff);
+    DBuf<int> err(1);
+    SPB_CUDA(cudaMemsetAsync(err.p, 0, sizeof(int), st));
+    dense::convert<double, float>(st, dscale, sc.p, (size_t)ncoeff);
+    const gram::Split z = gram::split_view(ws.p, (int)I1, (int)ncoeff);
+    gram::split(st, dA, sc.p, z);
+    for (uint64_t q0 = 0; q0 < I2; q0 += gram::kPanelRows)
+      gram::times(st, z, dB + q0 * ncoeff, (int)std::min<uint64_t>(gram::kPanelRows, I2 - q0), (size_t)ncoeff, 1,
+                  dscale, dC + q0, (size_t)I2, scr.p, err.p);
+    check_tc_err(st, err.p);
   });
 }
 
