@@ -25,6 +25,7 @@
 #include <mutex>
 
 #include "check.cuh"
+#include "s3ttmc_chain.cuh"
 #include "s3ttmc_tiled.cuh"
 #include "s3ttmc_warp.cuh"
 #include "tensor.cuh"
@@ -434,10 +435,13 @@ static PackedTables &tables_for(TensorState &t, uint32_t R) {
 }
 
 uint32_t s3ttmc_launch_count(const TensorState &t, uint32_t R, bool packed) {
-  (void)R;
   if (t.order <= 2) return packed ? 1 : 1;
-  uint32_t n = 1;                 // rows kernel
-  if (t.nsplit) n += 1;           // combine kernel
+  const bool chain = (s3ttmc_schedule() == kScheduleAuto || s3ttmc_schedule() == kScheduleChain) &&
+                     chain_supported(t, R);
+  const uint32_t nsplit = chain && t.chain ? t.chain->nsplit : t.nsplit;
+  uint32_t n = 1;                 // S3TTMc kernel
+  if (chain && t.chain && t.chain->nlight) n += 1;  // warp kernel of the light rows
+  if (nsplit) n += 1;             // combine kernel
   if (!packed) n += 1;            // unpack kernel
   return n;
 }
@@ -460,6 +464,48 @@ void unpack_rows(const void *dpacked, uint64_t rows, uint32_t dim, uint32_t orde
   spb_check_host(st, "unpack");
 }
 
+// A second stream of this device (created once, kept), forked from `st`
+// at construction: work queued on `side` starts after the work queued on
+// `st` so far, and join() makes later work on `st` wait for it.
+struct SideFork {
+  cudaStream_t st, side;
+  cudaEvent_t forked = nullptr, done = nullptr;
+  bool joined = false;
+  explicit SideFork(cudaStream_t s) : st(s) {
+    static std::mutex mu;
+    static std::map<int, cudaStream_t> sides;
+    int dev = 0;
+    SPB_CUDA(cudaGetDevice(&dev));
+    {
+      std::lock_guard<std::mutex> lock(mu);
+      auto it = sides.find(dev);
+      if (it == sides.end()) {
+        cudaStream_t x;
+        SPB_CUDA(cudaStreamCreateWithFlags(&x, cudaStreamNonBlocking));
+        it = sides.emplace(dev, x).first;
+      }
+      side = it->second;
+    }
+    SPB_CUDA(cudaEventCreateWithFlags(&forked, cudaEventDisableTiming));
+    SPB_CUDA(cudaEventCreateWithFlags(&done, cudaEventDisableTiming));
+    SPB_CUDA(cudaEventRecord(forked, st));
+    SPB_CUDA(cudaStreamWaitEvent(side, forked, 0));
+  }
+  void join() {
+    SPB_CUDA(cudaEventRecord(done, side));
+    SPB_CUDA(cudaStreamWaitEvent(st, done, 0));
+    joined = true;
+  }
+  ~SideFork() {
+    if (!joined) {  // an exception between fork and join: still order the streams
+      cudaEventRecord(done, side);
+      cudaStreamWaitEvent(st, done, 0);
+    }
+    cudaEventDestroy(forked);
+    cudaEventDestroy(done);
+  }
+};
+
 // One pass over a set of work items: writes the packed rows (or, when
 // `packed` is false, the full rows) [items.row0, items.row0 + items.rows) of
 // dY.  t.partials and t.scratch must already be large enough.
@@ -480,6 +526,36 @@ static void s3ttmc_items(TensorState &t, const ItemSet &items, const void *dU, u
   }
   void *Ypk = packed ? dY : (void *)t.scratch.p;
   const int sched = s3ttmc_schedule();
+  if (items.chain) {
+    // light rows on the warp-per-row kernel (the chain kernel where that
+    // kernel does not cover R), heavy rows on the chain kernel
+    if (items.nlight) {
+      ItemSet light;
+      light.chunks = items.light;
+      light.nchunks = items.nlight;
+      light.row0 = items.row0;
+      light.rows = items.rows;
+      auto it = t.warp.find(R);
+      if (it == t.warp.end()) it = t.warp.emplace(R, warp_plan(t.order, R)).first;
+      if (warp_supported(*it->second)) {
+        // the two kernels write disjoint rows: the light rows run on a side
+        // stream, forked from and joined back into `st`, beside the chain
+        // kernel (which leaves most issue slots idle)
+        SideFork fork(st);
+        warp_launch(*it->second, t, light, dU, Ypk, precision, fork.side);
+        chain_launch(t, *t.chain, items, dU, R, Ypk, precision, st);
+        fork.join();
+      } else {
+        light.chain = true;
+        chain_launch(t, *t.chain, light, dU, R, Ypk, precision, st);
+        chain_launch(t, *t.chain, items, dU, R, Ypk, precision, st);
+      }
+    } else {
+      chain_launch(t, *t.chain, items, dU, R, Ypk, precision, st);
+    }
+    finish_rows(t, items, m, Ypk, packed, dY, R, L, precision, st);
+    return;
+  }
   if (sched == kScheduleAuto || sched == kScheduleWarp) {
     auto it = t.warp.find(R);
     if (it == t.warp.end()) it = t.warp.emplace(R, warp_plan(t.order, R)).first;
@@ -545,6 +621,14 @@ static void s3ttmc_items(TensorState &t, const ItemSet &items, const void *dU, u
 
 // make room for the partial sums of split rows and, for full output, the
 // packed staging rows
+// whether this call runs the pivot-chain schedule
+static bool use_chain(const TensorState &t, uint32_t R) {
+  const int sched = s3ttmc_schedule();
+  if (sched == kScheduleChain && !chain_supported(t, R))
+    fail(SYMPROP_ERR_SIZE, "chain S3TTMc does not support order %u rank %u", t.order, R);
+  return (sched == kScheduleAuto || sched == kScheduleChain) && chain_supported(t, R);
+}
+
 static void s3ttmc_reserve(TensorState &t, uint32_t R, bool packed, int precision) {
   if (R == 0) fail(SYMPROP_ERR_INVALID, "R must be positive");
   if (precision != SYMPROP_FP64 && precision != SYMPROP_FP32)
@@ -552,7 +636,9 @@ static void s3ttmc_reserve(TensorState &t, uint32_t R, bool packed, int precisio
   const size_t es = precision == SYMPROP_FP64 ? 8 : 4;
   const uint64_t m = symsize(R, t.order - 1);
   if (!packed && t.order > 2) t.scratch.ensure((size_t)t.dim * m * es);
-  if (t.nslots) t.partials.ensure((size_t)t.nslots * m);
+  uint32_t slots = t.nslots;
+  if (use_chain(t, R)) slots = std::max(slots, chain_data(t).nslots);
+  if (slots) t.partials.ensure((size_t)slots * m);
 }
 
 void s3ttmc_run(TensorState &t, const void *dU, uint32_t R, bool packed, void *dY, int precision,
@@ -560,10 +646,23 @@ void s3ttmc_run(TensorState &t, const void *dU, uint32_t R, bool packed, void *d
   NvtxRange nv("S3TTMc");
   s3ttmc_reserve(t, R, packed, precision);
   ItemSet all;
-  all.chunks = t.chunks.p;
-  all.nchunks = t.nchunks;
-  all.split = t.split.p;
-  all.nsplit = t.nsplit;
+  if (use_chain(t, R)) {
+    const ChainData &cd = chain_data(t);
+    all.chunks = cd.chunks.p;
+    all.nchunks = cd.nchunks;
+    all.split = cd.split.p;
+    all.nsplit = cd.nsplit;
+    all.chain = true;
+    all.nslots = cd.nslots;
+    all.light = cd.light.p;
+    all.nlight = cd.nlight;
+  } else {
+    all.chunks = t.chunks.p;
+    all.nchunks = t.nchunks;
+    all.split = t.split.p;
+    all.nsplit = t.nsplit;
+    all.nslots = t.nslots;
+  }
   all.row0 = 0;
   all.rows = t.dim;
   s3ttmc_items(t, all, dU, R, packed, dY, precision, st);
@@ -614,7 +713,8 @@ void s3ttmc_host(TensorState &t, const void *U, uint32_t R, bool packed, void *Y
   const size_t ubytes = (size_t)t.dim * R * es, ybytes = (size_t)t.dim * cols * es;
   t.io_U.ensure(ubytes);
   t.io_Y.ensure(ybytes);
-  const RowBands &bd = row_bands(t, host_band_count(ybytes));
+  const bool chain = use_chain(t, R);
+  const RowBands &bd = chain ? chain_bands(t, host_band_count(ybytes)) : row_bands(t, host_band_count(ybytes));
 
   // SPB_TRACE_HOST=1 prints when each band's compute and copy ended
   const bool trace = std::getenv("SPB_TRACE_HOST") != nullptr;
@@ -651,6 +751,12 @@ void s3ttmc_host(TensorState &t, const void *U, uint32_t R, bool packed, void *Y
     band.nsplit = bd.split0[k + 1] - bd.split0[k];
     band.row0 = bd.row0[k];
     band.rows = bd.row0[k + 1] - bd.row0[k];
+    band.chain = chain;
+    band.nslots = chain ? t.chain->nslots : t.nslots;
+    if (chain) {
+      band.light = bd.light.p + bd.light0[k];
+      band.nlight = bd.light0[k + 1] - bd.light0[k];
+    }
     s3ttmc_items(t, band, t.io_U.p, R, packed, t.io_Y.p, precision, ss.st);
     SPB_CUDA(cudaEventRecord(ss.done[k], ss.st));
   }
@@ -683,10 +789,10 @@ static void finish_rows(TensorState &t, const ItemSet &items, uint64_t m, void *
     dim3 grid(items.nsplit, (unsigned)((m + 31) / 32));
     if (precision == SYMPROP_FP64)
       combine_kernel<double><<<grid, 256, 0, st>>>(items.split, t.partials.p, (uint32_t)m, Ypk, m, t.dim,
-                                                   t.nslots);
+                                                   items.nslots);
     else
       combine_kernel<float><<<grid, 256, 0, st>>>(items.split, t.partials.p, (uint32_t)m, Ypk, m, t.dim,
-                                                  t.nslots);
+                                                  items.nslots);
     SPB_LAUNCH_CHECK();
   }
   if (!packed && items.rows) {

@@ -1,0 +1,608 @@
+// S3TTMc, pivot-chain schedule (order 4 / R <= 16): the owners of a row are
+// contracted pivot by pivot instead of leaf by leaf.
+//
+// The reference's leaf tensor (SymOuterProd recursion,
+// include/detail/dense/symtensor.hpp:24-39, src/compressed_dtree.cpp:421-518)
+// is, for a leaf S = {s_1, s_2, s_3} and sorted column indices q,
+//     K(S)[q0 q1 q2] = sum over the 6 orderings of S of prod_k U[s_pi(k)][q_k]
+//                    = sum_t U[s_1][q_t] * K({s_2, s_3})[q without q_t]
+// for any choice of the position s_1, and K({s_2, s_3})[x, y] =
+// U[s_2][x] U[s_3][y] + U[s_3][x] U[s_2][y].  With every leaf ordered by node
+// degree (s_1 the node of highest degree) and a row's owners sorted by
+// (s_1, s_2), the row is
+//     Y[i] = Sym3(G),   G = sum_{s_1} U[s_1] (x) Q_{s_1}                (16 x m2)
+//     Q_{s_1} = sum_{s_2} U[s_2] (x)s W_{s_1 s_2}                         (m2 = R(R+1)/2)
+//     W_{s_1 s_2} = sum over its owners of c * U[s_3]                     (R)
+// with Sym3(G)[q0 q1 q2] = G[q0][q1 q2] + G[q1][q0 q2] + G[q2][q0 q1] and
+// (x)s the symmetric outer product.  Hub rows share their high-degree
+// pivots across many owners: on the order-4 Zipf(1.1) workload a row has
+// 0.11 distinct s_1 and 0.50 distinct (s_1, s_2) per owner, so the row
+// costs about 16 + 0.50 * 272 + 0.11 * 2176 FMAs per owner, against about
+// 3,300 for the leaf-by-leaf schedule.  The sums are the reference's,
+// associated differently (FP64 results agree to rounding).
+//
+// Kernel: one CTA of 128 threads per work item (a row, or a slice of a long
+// row whose partial rows the combine kernel adds).  Owners are taken in
+// batches of up to 256 with at most kSG (s_1, s_2) subgroups and kG s_1
+// groups (43 KB of shared memory in FP64: 4 CTAs per SM); a batch boundary (or slice boundary) may cut a group: by
+// linearity the two parts add up.  Per batch: W of every subgroup, then Q of
+// every group (shared memory), then each thread adds its 18 entries of G.
+// The row's G then goes through shared memory for Sym3.  FP32: the batch's
+// G is summed in FP32 and folded into FP64 totals after every batch.
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <map>
+#include <mutex>
+
+#include "check.cuh"
+#include "s3ttmc_chain.cuh"
+
+namespace spb {
+namespace {
+
+constexpr int kThreads = 128;
+constexpr int kB = 256;   // owners per batch
+constexpr int kSG = 64;   // (s_1, s_2) subgroups per batch
+constexpr int kG = 16;    // s_1 groups per batch
+constexpr int kRP = 16;   // R padded
+constexpr int kM2 = 136;  // packed order-2 entries at R = 16
+constexpr int kBeta = 9;  // beta slots per thread: 16 x 9 >= kM2
+
+struct ChainParams {
+  const Chunk *chunks;
+  uint32_t nchunks;
+  const uint32_t *S;  // nown x sstride, leaf ids in pivot order
+  uint32_t sstride;
+  const void *c;      // coefficients (T)
+  const uint8_t *flags;
+  const void *U;      // n x R (T)
+  uint32_t R, m2, m3;
+  void *Y;            // packed rows (T), row stride m3
+  double *partials;   // nslots x m3
+  const uint32_t *trip;  // m3 packed (q0 | q1 << 8 | q2 << 16), lexicographic
+  uint64_t nown;
+  uint32_t nrows, nslots;
+};
+
+__device__ __forceinline__ uint32_t pair_index(uint32_t x, uint32_t y, uint32_t R) {  // x <= y
+  return x * R - (x * (x - 1)) / 2 + (y - x);
+}
+
+template <typename T> struct Smem {
+  uint32_t s1[kB], s2[kB], s3[kB];
+  uint8_t px[kM2], py[kM2];  // packed order-2 index -> (x <= y)
+  T c[kB];
+  uint16_t sg_start[kSG + 1], g_sg[kG + 1];
+  uint32_t sg_s2[kSG], g_s1[kG];
+  uint32_t warp_tot[kThreads / 32];
+  int nb, nsg, ng;
+  union {
+    struct {
+      T W[kSG][kRP], U2[kSG][kRP];
+      T Q[kG][kM2];
+      T U1[kG][kRP];
+    } b;                        // one batch
+    double G[kRP * kM2];        // the row's G at the end (FP64)
+  } u;
+};
+
+// Inclusive scan over the CTA of 32-bit values (two 16-bit counts packed).
+__device__ __forceinline__ uint32_t cta_scan(uint32_t v, uint32_t *warp_tot) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const uint32_t u = __shfl_up_sync(0xffffffffu, v, d);
+    if (lane >= d) v += u;
+  }
+  if (lane == 31) warp_tot[warp] = v;
+  __syncthreads();
+  uint32_t off = 0;
+  for (int w = 0; w < warp; ++w) off += warp_tot[w];
+  return v + off;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kThreads, 4) s3ttmc_chain_kernel(const ChainParams p) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Smem<T> &sm = *reinterpret_cast<Smem<T> *>(smem_raw);
+  const int tid = threadIdx.x;
+  const Chunk ch = p.chunks[blockIdx.x];
+  if (!SPB_BOUND(ch.ob <= ch.oe && ch.oe <= p.nown && ch.row < p.nrows && (ch.slot == kDirect || ch.slot < p.nslots),
+                 201, blockIdx.x))
+    return;  // the whole CTA leaves
+  const T *U = reinterpret_cast<const T *>(p.U);
+  const T *cc = reinterpret_cast<const T *>(p.c);
+  const uint32_t R = p.R, m2 = p.m2;
+
+  for (uint32_t b = tid; b < m2; b += kThreads) {  // lexicographic pairs
+    uint32_t x = 0, rem = b;
+    while (rem >= R - x) {
+      rem -= R - x;
+      ++x;
+    }
+    sm.px[b] = (uint8_t)x;
+    sm.py[b] = (uint8_t)(x + rem);
+  }
+  __syncthreads();
+  // this thread's entries of G: rows a0, a0 + 1, columns b0 + 16 k
+  const int a0 = 2 * (tid & 7), b0 = tid >> 3;
+  double gsum[2][kBeta];
+#pragma unroll
+  for (int a = 0; a < 2; ++a)
+#pragma unroll
+    for (int k = 0; k < kBeta; ++k) gsum[a][k] = 0.0;
+
+  // owner records of the window [o, o + kB): thread t holds owners 2t, 2t+1;
+  // the next window is fetched while the current batch is computed
+  struct Rec {
+    uint4 ids;
+    T c;
+    uint32_t f;
+  };
+  auto fetch = [&](uint64_t w0, Rec (&r)[2]) {
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const uint64_t o = w0 + (uint64_t)(2 * tid + h);
+      if (o < ch.oe) {
+        r[h].ids = *reinterpret_cast<const uint4 *>(p.S + o * p.sstride);
+        r[h].c = cc[o];
+        r[h].f = p.flags[o];
+      }
+    }
+  };
+  Rec rec[2];
+  fetch(ch.ob, rec);
+  for (uint64_t o0 = ch.ob; o0 < ch.oe;) {
+    const uint64_t left = ch.oe - o0;
+    // ---- batch: the window's owners, counts of group and subgroup starts
+    // (packed: subgroup starts << 16 | group starts)
+    uint32_t fl[2] = {0u, 0u};
+    bool in[2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int i = 2 * tid + h;
+      in[h] = (uint64_t)i < left;
+      if (in[h]) {
+        uint4 ids = rec[h].ids;
+        if (!SPB_BOUND(ids.x < p.nrows && ids.y < p.nrows && ids.z < p.nrows, 202, o0 + (uint64_t)i))
+          ids = make_uint4(0, 0, 0, 0);
+        sm.s1[i] = ids.x;
+        sm.s2[i] = ids.y;
+        sm.s3[i] = ids.z;
+        sm.c[i] = rec[h].c;
+        uint32_t f = rec[h].f;
+        if (i == 0) f = 3u;  // a batch starts a group and a subgroup
+        fl[h] = (f & 1u) | (((f >> 1) & 1u) << 16);
+      }
+    }
+    const uint32_t c1 = cta_scan(fl[0] + fl[1], sm.warp_tot);  // counts through owner 2t+1
+    const uint32_t c0 = c1 - fl[1];                            // counts through owner 2t
+    const uint32_t cnt[2] = {c0, c1};
+    auto within = [](uint32_t c) { return (c & 0xffffu) <= (uint32_t)kG && (c >> 16) <= (uint32_t)kSG; };
+    const bool v[2] = {in[0] && within(c0), in[1] && within(c1)};
+    // The batch is the first nb owners (validity is a prefix: the counts
+    // grow along the owners).  Exactly one thread sees the boundary: owner
+    // 2t - 1 valid and 2t not, 2t valid and 2t + 1 not, or all 256 valid.
+    const bool prev_valid = tid > 0 && (uint64_t)(2 * tid - 1) < left && within(c0 - fl[0]);
+    if (!v[0] && prev_valid) sm.nb = 2 * tid;
+    if (v[0] && !v[1]) sm.nb = 2 * tid + 1;
+    if (v[1] && tid == kThreads - 1) sm.nb = kB;
+    __syncthreads();
+    const int nb = sm.nb;
+    fetch(o0 + (uint64_t)nb, rec);  // in flight during this batch
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      if (!v[h]) continue;
+      const int i = 2 * tid + h;
+      const uint32_t g = cnt[h] & 0xffffu, sg = cnt[h] >> 16;
+      if (fl[h] >> 16) {
+        sm.sg_start[sg - 1] = (uint16_t)i;
+        sm.sg_s2[sg - 1] = sm.s2[i];
+      }
+      if (fl[h] & 0xffffu) {
+        sm.g_sg[g - 1] = (uint16_t)(sg - 1);
+        sm.g_s1[g - 1] = sm.s1[i];
+      }
+      if (i == nb - 1) {
+        sm.nsg = (int)sg;
+        sm.ng = (int)g;
+        sm.sg_start[sg] = (uint16_t)nb;
+        sm.g_sg[g] = (uint16_t)sg;
+      }
+    }
+    __syncthreads();
+    const int nsg = sm.nsg, ng = sm.ng;
+    // ---- W of every subgroup (and its s_2 row of U)
+    {
+      const int x = tid & 15;
+      for (int sg = tid >> 4; sg < nsg; sg += kThreads / 16) {
+        T w = T(0), u2 = T(0);
+        if ((uint32_t)x < R) {
+#pragma unroll 4
+          for (int i = sm.sg_start[sg]; i < sm.sg_start[sg + 1]; ++i) w += sm.c[i] * U[(uint64_t)sm.s3[i] * R + x];
+          u2 = U[(uint64_t)sm.sg_s2[sg] * R + x];
+        }
+        sm.u.b.W[sg][x] = w;
+        sm.u.b.U2[sg][x] = u2;
+      }
+      for (int g = tid >> 4; g < ng; g += kThreads / 16)
+        sm.u.b.U1[g][x] = (uint32_t)x < R ? U[(uint64_t)sm.g_s1[g] * R + x] : T(0);
+    }
+    __syncthreads();
+    // ---- Q of every group: sum over its subgroups of U2 (x)s W
+    for (int e = tid; e < ng * (int)m2; e += kThreads) {
+      const int g = e / (int)m2, b = e - g * (int)m2;
+      const uint32_t x = sm.px[b], y = sm.py[b];
+      T q = T(0);
+      for (int sg = sm.g_sg[g]; sg < sm.g_sg[g + 1]; ++sg) q += sm.u.b.U2[sg][x] * sm.u.b.W[sg][y] + sm.u.b.W[sg][x] * sm.u.b.U2[sg][y];
+      sm.u.b.Q[g][b] = q;
+    }
+    __syncthreads();
+    // ---- G += U1 (x) Q over the batch's groups
+    {
+      T acc[2][kBeta];
+#pragma unroll
+      for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int k = 0; k < kBeta; ++k) acc[a][k] = T(0);
+      for (int g = 0; g < ng; ++g) {
+        const T u0 = sm.u.b.U1[g][a0], u1 = sm.u.b.U1[g][a0 + 1];
+#pragma unroll
+        for (int k = 0; k < kBeta; ++k) {
+          const int b = b0 + 16 * k;
+          const T q = b < (int)m2 ? sm.u.b.Q[g][b] : T(0);
+          acc[0][k] += u0 * q;
+          acc[1][k] += u1 * q;
+        }
+      }
+#pragma unroll
+      for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int k = 0; k < kBeta; ++k) gsum[a][k] += (double)acc[a][k];
+    }
+    o0 += (uint64_t)sm.nb;
+    __syncthreads();
+  }
+  // ---- Y = Sym3(G) through shared memory (FP64)
+  double *sG = reinterpret_cast<double *>(&sm.u.b.W[0][0]);  // kRP x kM2
+#pragma unroll
+  for (int a = 0; a < 2; ++a)
+#pragma unroll
+    for (int k = 0; k < kBeta; ++k) {
+      const int b = b0 + 16 * k;
+      if (b < kM2) sG[(a0 + a) * kM2 + b] = gsum[a][k];
+    }
+  __syncthreads();
+  T *Yrow = reinterpret_cast<T *>(p.Y) + (uint64_t)ch.row * p.m3;
+  double *Prow = p.partials + (uint64_t)ch.slot * p.m3;
+  for (uint32_t e = tid; e < p.m3; e += kThreads) {
+    const uint32_t t3 = p.trip[e];
+    const uint32_t q0 = t3 & 0xffu, q1 = (t3 >> 8) & 0xffu, q2 = t3 >> 16;
+    const double y = sG[q0 * kM2 + pair_index(q1, q2, R)] + sG[q1 * kM2 + pair_index(q0, q2, R)] +
+                     sG[q2 * kM2 + pair_index(q0, q1, R)];
+    if (ch.slot == kDirect) Yrow[e] = (T)y;
+    else Prow[e] = y;
+  }
+}
+
+// ---------------------------------------------------------------- build
+
+__global__ void degree_kernel(const uint32_t *inds0, uint64_t n, uint32_t *deg) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    atomicAdd(&deg[inds0[i]], 1u);
+}
+
+__global__ void desc_key_kernel(const uint32_t *deg, uint32_t n, uint32_t *key) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) key[i] = ~deg[i];  // ascending key = descending degree
+}
+
+__global__ void rank_kernel(const uint32_t *by_degree, uint32_t n, uint32_t *rank) {
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n) rank[by_degree[k]] = k;
+}
+
+// row of every owner: the last i with row_ptr[i] <= o
+__global__ void owner_row_kernel(const uint64_t *row_ptr, uint32_t dim, uint64_t nown, uint32_t *own_row) {
+  const uint64_t o = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (o >= nown) return;
+  uint32_t lo = 0, hi = dim;  // row_ptr[lo] <= o < row_ptr[hi]
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (row_ptr[mid] <= o) lo = mid; else hi = mid;
+  }
+  own_row[o] = lo;
+}
+
+// Leaf ids in pivot order (ascending degree rank) and the sort key of the
+// first L-1 pivots (most significant first).
+__global__ void pivot_order_kernel(const uint32_t *S, uint64_t nown, uint32_t sstride, uint32_t L, const uint32_t *rank,
+                                   int bits, uint32_t *S_out, uint64_t *key) {
+  const uint64_t o = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (o >= nown) return;
+  uint32_t id[8], rk[8];
+  for (uint32_t k = 0; k < L; ++k) {
+    id[k] = S[o * sstride + k];
+    rk[k] = rank[id[k]];
+  }
+  for (uint32_t a = 1; a < L; ++a) {  // insertion sort by rank
+    const uint32_t vi = id[a], vr = rk[a];
+    int b = (int)a - 1;
+    while (b >= 0 && rk[b] > vr) {
+      id[b + 1] = id[b];
+      rk[b + 1] = rk[b];
+      --b;
+    }
+    id[b + 1] = vi;
+    rk[b + 1] = vr;
+  }
+  uint64_t kv = 0;
+  for (uint32_t k = 0; k + 1 < L; ++k) kv = (kv << bits) | rk[k];
+  key[o] = kv;
+  for (uint32_t k = 0; k < sstride; ++k) S_out[o * sstride + k] = k < L ? id[k] : 0u;
+}
+
+__global__ void gather_rows_kernel(const uint32_t *perm, const uint32_t *own_row, uint64_t n, uint32_t *out) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = own_row[perm[i]];
+}
+
+__global__ void chain_gather_kernel(const uint32_t *perm, uint64_t nown, uint32_t sstride, const uint32_t *S_in,
+                                    const double *c_in, uint32_t *S_out, double *c64, float *c32) {
+  const uint64_t o = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (o >= nown) return;
+  const uint32_t src = perm[o];
+  for (uint32_t k = 0; k < sstride; ++k) S_out[o * sstride + k] = S_in[(uint64_t)src * sstride + k];
+  c64[o] = c_in[src];
+  c32[o] = (float)c_in[src];
+}
+
+// bit k: owner o starts a new prefix of k + 1 pivots (a new row starts all)
+__global__ void chain_flags_kernel(const uint32_t *S, const uint32_t *row_sorted, uint64_t nown, uint32_t sstride,
+                                   uint32_t L, uint8_t *flags) {
+  const uint64_t o = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (o >= nown) return;
+  uint32_t f = 0;
+  if (o == 0 || row_sorted[o] != row_sorted[o - 1]) {
+    f = 0xffu;
+  } else {
+    bool differ = false;
+    for (uint32_t k = 0; k + 1 < L; ++k) {
+      differ = differ || S[o * sstride + k] != S[(o - 1) * sstride + k];
+      if (differ) f |= 1u << k;
+    }
+  }
+  flags[o] = (uint8_t)f;
+}
+
+inline unsigned blocks_for(uint64_t n, unsigned b) { return (unsigned)std::max<uint64_t>(1, (n + b - 1) / b); }
+
+template <class V> void upload(DBuf<V> &d, const std::vector<V> &h) {
+  d.alloc(h.size());
+  if (!h.empty()) SPB_CUDA(cudaMemcpy(d.p, h.data(), h.size() * sizeof(V), cudaMemcpyHostToDevice));
+}
+
+uint64_t heavy_owner_count(const TensorState &t) {
+  uint64_t s = 0;
+  for (uint32_t i = 0; i < t.dim; ++i) {
+    const uint64_t c = t.h_row_ptr[i + 1] - t.h_row_ptr[i];
+    if (c > kChainLight) s += c;
+  }
+  return s;
+}
+
+// Items of rows [r0, r1) in row order: rows of at most kChainLight owners
+// as one light item each, heavier rows as chain items of at most co owners
+// (a row of several items gets partial-sum slots).  Returns the slot count.
+uint32_t cut_chain_rows(const TensorState &t, uint64_t co, uint32_t r0, uint32_t r1, std::vector<Chunk> &ch,
+                        std::vector<SplitRow> &sp, std::vector<Chunk> &lt) {
+  ch.clear();
+  sp.clear();
+  lt.clear();
+  uint32_t slot = 0;
+  for (uint32_t i = r0; i < r1; ++i) {
+    const uint64_t b = t.h_row_ptr[i], e = t.h_row_ptr[(size_t)i + 1];
+    if (e - b <= kChainLight) {
+      lt.push_back(Chunk{i, kDirect, b, e});
+    } else if (e - b <= co) {
+      ch.push_back(Chunk{i, kDirect, b, e});
+    } else {
+      const uint32_t s0 = slot;
+      for (uint64_t x = b; x < e; x += co) ch.push_back(Chunk{i, slot++, x, std::min(e, x + co)});
+      sp.push_back(SplitRow{i, s0, slot, 0});
+    }
+  }
+  return slot;
+}
+
+}  // namespace
+
+bool chain_supported(const TensorState &t, uint32_t R) {
+  return t.order == 4 && R >= 1 && R <= (uint32_t)kRP && t.dim < (1u << 24) && t.nown < (1ull << 32);
+}
+
+ChainData &chain_data(TensorState &t) {
+  if (t.chain) return *t.chain;
+  NvtxRange nv("chain build");
+  auto cd = std::make_shared<ChainData>();
+  const uint32_t L = t.order - 1, n = t.dim;
+  const uint64_t nown = t.nown;
+  cd->L = L;
+  cudaStream_t st = 0;
+  // degree rank of every node (0 = most frequent; ties by id)
+  DBuf<uint32_t> deg(n), key(n), key_sorted(n), ids(n), by_degree(n), rank(n);
+  SPB_CUDA(cudaMemsetAsync(deg.p, 0, sizeof(uint32_t) * n, st));
+  if (t.nnz) {
+    degree_kernel<<<blocks_for(t.nnz * t.order, 256), 256, 0, st>>>(t.inds.p, t.nnz * t.order, deg.p);
+    SPB_LAUNCH_CHECK();
+  }
+  desc_key_kernel<<<blocks_for(n, 256), 256, 0, st>>>(deg.p, n, key.p);
+  SPB_LAUNCH_CHECK();
+  device_iota(ids.p, n, st);
+  {
+    size_t tmp = 0;
+    SPB_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, key.p, key_sorted.p, ids.p, by_degree.p, n, 0, 32, st));
+    DBuf<char> work(std::max<size_t>(tmp, 1));
+    SPB_CUDA(cub::DeviceRadixSort::SortPairs(work.p, tmp, key.p, key_sorted.p, ids.p, by_degree.p, n, 0, 32, st));
+  }
+  rank_kernel<<<blocks_for(n, 256), 256, 0, st>>>(by_degree.p, n, rank.p);
+  SPB_LAUNCH_CHECK();
+  deg.release();
+  key.release();
+  key_sorted.release();
+  ids.release();
+  by_degree.release();
+
+  // owners: leaves in pivot order; stable sort by the pivot key, then by row
+  const int bits = bits_for(n ? n - 1 : 0);
+  const int key_bits = bits * (int)(L - 1);
+  if (key_bits > 64) fail(SYMPROP_ERR_SIZE, "chain schedule: pivot key of %d bits", key_bits);
+  DBuf<uint32_t> S_piv(nown * t.sstride), own_row(nown), perm_a(nown), perm_b(nown), rows_a(nown), rows_b(nown);
+  DBuf<uint64_t> pkey(nown), pkey_sorted(nown);
+  if (nown) {
+    pivot_order_kernel<<<blocks_for(nown, 256), 256, 0, st>>>(t.own_S.p, nown, t.sstride, L, rank.p, bits, S_piv.p,
+                                                               pkey.p);
+    SPB_LAUNCH_CHECK();
+    owner_row_kernel<<<blocks_for(nown, 256), 256, 0, st>>>(t.row_ptr.p, n, nown, own_row.p);
+    SPB_LAUNCH_CHECK();
+    device_iota(perm_a.p, nown, st);
+    size_t tmp1 = 0, tmp2 = 0;
+    SPB_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp1, pkey.p, pkey_sorted.p, perm_a.p, perm_b.p, nown, 0,
+                                             std::max(key_bits, 1), st));
+    SPB_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp2, rows_a.p, rows_b.p, perm_b.p, perm_a.p, nown, 0,
+                                             bits_for(n), st));
+    DBuf<char> work(std::max<size_t>(std::max(tmp1, tmp2), 1));
+    SPB_CUDA(cub::DeviceRadixSort::SortPairs(work.p, tmp1, pkey.p, pkey_sorted.p, perm_a.p, perm_b.p, nown, 0,
+                                             std::max(key_bits, 1), st));
+    gather_rows_kernel<<<blocks_for(nown, 256), 256, 0, st>>>(perm_b.p, own_row.p, nown, rows_a.p);
+    SPB_LAUNCH_CHECK();
+    SPB_CUDA(cub::DeviceRadixSort::SortPairs(work.p, tmp2, rows_a.p, rows_b.p, perm_b.p, perm_a.p, nown, 0,
+                                             bits_for(n), st));
+  }
+  cd->S.alloc(nown * t.sstride);
+  cd->c64.alloc(nown);
+  cd->c32.alloc(nown);
+  cd->flags.alloc(nown);
+  if (nown) {
+    chain_gather_kernel<<<blocks_for(nown, 256), 256, 0, st>>>(perm_a.p, nown, t.sstride, S_piv.p, t.own_c64.p, cd->S.p,
+                                                               cd->c64.p, cd->c32.p);
+    SPB_LAUNCH_CHECK();
+    chain_flags_kernel<<<blocks_for(nown, 256), 256, 0, st>>>(cd->S.p, rows_b.p, nown, t.sstride, L, cd->flags.p);
+    SPB_LAUNCH_CHECK();
+  }
+  // work items: the rows' owner ranges are unchanged (the sort keeps rows);
+  // light rows one item each, heavy rows cut into items of at most co owners
+  const uint64_t heavy_owners = heavy_owner_count(t);
+  const uint64_t target_items = 148ull * 4ull * 8ull;
+  uint64_t co = (heavy_owners + target_items - 1) / target_items;
+  co = std::min<uint64_t>(std::max<uint64_t>(co, 256), 1024);
+  cd->chunk_owners = (uint32_t)co;
+  std::vector<Chunk> ch, lt;
+  std::vector<SplitRow> sp;
+  cd->nslots = cut_chain_rows(t, co, 0, t.dim, ch, sp, lt);
+  sort_heaviest_first(ch, 0, ch.size(), co);
+  sort_heaviest_first(lt, 0, lt.size(), kChainLight);
+  cd->nchunks = (uint32_t)ch.size();
+  cd->nsplit = (uint32_t)sp.size();
+  cd->nlight = (uint32_t)lt.size();
+  upload(cd->chunks, ch);
+  upload(cd->split, sp);
+  upload(cd->light, lt);
+  SPB_CUDA(cudaDeviceSynchronize());
+  t.chain = cd;
+  return *cd;
+}
+
+const RowBands &chain_bands(TensorState &t, uint32_t nb) {
+  ChainData &cd = chain_data(t);
+  nb = std::max<uint32_t>(1, std::min<uint32_t>(nb, std::max<uint32_t>(t.dim, 1)));
+  auto found = cd.bands.find(nb);
+  if (found != cd.bands.end()) return *found->second;
+  auto b = std::make_unique<RowBands>();
+  b->nb = nb;
+  std::vector<Chunk> ch, lt;
+  std::vector<SplitRow> sp;
+  cut_chain_rows(t, cd.chunk_owners, 0, t.dim, ch, sp, lt);
+  b->row0.resize(nb + 1);
+  b->chunk0.resize(nb + 1);
+  b->split0.resize(nb + 1);
+  b->light0.resize(nb + 1);
+  for (uint32_t k = 0; k <= nb; ++k) {
+    const uint32_t r = (uint32_t)((uint64_t)t.dim * k / nb);
+    b->row0[k] = r;
+    auto before = [r](const auto &v) {
+      return (uint32_t)(std::lower_bound(v.begin(), v.end(), r, [](const auto &c, uint32_t x) { return c.row < x; }) -
+                        v.begin());
+    };
+    b->chunk0[k] = before(ch);
+    b->split0[k] = before(sp);
+    b->light0[k] = before(lt);
+  }
+  for (uint32_t k = 0; k < nb; ++k) {
+    sort_heaviest_first(ch, b->chunk0[k], b->chunk0[k + 1], cd.chunk_owners);
+    sort_heaviest_first(lt, b->light0[k], b->light0[k + 1], kChainLight);
+  }
+  upload(b->chunks, ch);
+  upload(b->split, sp);
+  upload(b->light, lt);
+  return *(cd.bands[nb] = std::move(b));
+}
+
+namespace {
+// lexicographic sorted triples of [0, R), packed 8 bits each (per R, kept)
+const uint32_t *triples(uint32_t R) {
+  static std::mutex mu;
+  // kept for the life of the process (a few KB per rank and device)
+  static std::map<std::pair<int, uint32_t>, uint32_t *> cache;
+  int dev = 0;
+  SPB_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(mu);
+  uint32_t *&slot = cache[{dev, R}];
+  if (!slot) {
+    std::vector<uint32_t> h;
+    for_each_sorted(R, 3, [&](const std::vector<uint32_t> &q, uint64_t) { h.push_back(q[0] | q[1] << 8 | q[2] << 16); });
+    uint32_t *d = nullptr;
+    SPB_CUDA(cudaMalloc(&d, h.size() * sizeof(uint32_t)));
+    SPB_CUDA(cudaMemcpy(d, h.data(), h.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    slot = d;
+  }
+  return slot;
+}
+}  // namespace
+
+void chain_launch(const TensorState &t, const ChainData &cd, const ItemSet &items, const void *dU, uint32_t R,
+                  void *dYpacked, int precision, cudaStream_t st) {
+  if (!chain_supported(t, R)) fail(SYMPROP_ERR_SIZE, "chain S3TTMc does not support order %u rank %u", t.order, R);
+  if (!items.nchunks) return;
+  ChainParams p;
+  p.chunks = items.chunks;
+  p.nchunks = items.nchunks;
+  p.S = cd.S.p;
+  p.sstride = t.sstride;
+  p.c = precision == SYMPROP_FP64 ? (const void *)cd.c64.p : (const void *)cd.c32.p;
+  p.flags = cd.flags.p;
+  p.U = dU;
+  p.R = R;
+  p.m2 = R * (R + 1) / 2;
+  p.m3 = (uint32_t)symsize(R, 3);
+  p.Y = dYpacked;
+  p.partials = t.partials.p;
+  p.trip = triples(R);
+  p.nown = t.nown;
+  p.nrows = t.dim;
+  p.nslots = cd.nslots;
+  if (precision == SYMPROP_FP64) {
+    const size_t smem = sizeof(Smem<double>);
+    SPB_CUDA(cudaFuncSetAttribute(s3ttmc_chain_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    s3ttmc_chain_kernel<double><<<items.nchunks, kThreads, smem, st>>>(p);
+  } else {
+    const size_t smem = sizeof(Smem<float>);
+    SPB_CUDA(cudaFuncSetAttribute(s3ttmc_chain_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    s3ttmc_chain_kernel<float><<<items.nchunks, kThreads, smem, st>>>(p);
+  }
+  SPB_LAUNCH_CHECK();
+  spb_check_host(st, "S3TTMc chain kernel");
+}
+
+}  // namespace spb

@@ -134,17 +134,17 @@ inline unsigned grid_for(uint64_t n, unsigned block) {
 
 }  // namespace
 
-// The work items in row order: one chunk per row, rows with more than
-// t.chunk_owners owners cut into consecutive slices, each slice with its own
-// partial-sum slot.  Returns the number of slots.
-static uint32_t row_order_items(const TensorState &t, std::vector<Chunk> &ch, std::vector<SplitRow> &sp) {
-  const uint64_t co = t.chunk_owners;
+// The work items in row order: one chunk per row, rows with more than co
+// owners cut into consecutive slices, each slice with its own partial-sum
+// slot.  Returns the number of slots.
+uint32_t cut_rows(const std::vector<uint64_t> &row_ptr, uint32_t dim, uint64_t co, std::vector<Chunk> &ch,
+                  std::vector<SplitRow> &sp) {
   ch.clear();
   sp.clear();
-  ch.reserve((size_t)t.dim + t.nown / co + 1);
+  ch.reserve((size_t)dim + row_ptr[dim] / co + 1);
   uint32_t slot = 0;
-  for (uint32_t i = 0; i < t.dim; ++i) {
-    uint64_t b = t.h_row_ptr[i], e = t.h_row_ptr[(size_t)i + 1];
+  for (uint32_t i = 0; i < dim; ++i) {
+    uint64_t b = row_ptr[i], e = row_ptr[(size_t)i + 1];
     uint64_t c = e - b;
     if (c <= co) {
       ch.push_back(Chunk{i, kDirect, b, e});
@@ -157,9 +157,13 @@ static uint32_t row_order_items(const TensorState &t, std::vector<Chunk> &ch, st
   return slot;
 }
 
+static uint32_t row_order_items(const TensorState &t, std::vector<Chunk> &ch, std::vector<SplitRow> &sp) {
+  return cut_rows(t.h_row_ptr, t.dim, t.chunk_owners, ch, sp);
+}
+
 // Stable sort of ch[b, e) by owner count, heaviest first: a counting sort,
 // since no chunk holds more than max_owners owners.
-static void sort_heaviest_first(std::vector<Chunk> &ch, size_t b, size_t e, uint64_t max_owners) {
+void sort_heaviest_first(std::vector<Chunk> &ch, size_t b, size_t e, uint64_t max_owners) {
   std::vector<size_t> start(max_owners + 2, 0);
   for (size_t i = b; i < e; ++i) ++start[max_owners - (ch[i].oe - ch[i].ob) + 1];
   for (size_t k = 1; k < start.size(); ++k) start[k] += start[k - 1];
@@ -306,6 +310,7 @@ void tensor_build(TensorState &t, const uint32_t *h_inds, const double *h_vals, 
   if (!sp.empty())
     SPB_CUDA(cudaMemcpy(t.split.p, sp.data(), sp.size() * sizeof(SplitRow), cudaMemcpyHostToDevice));
   t.bands.clear();
+  t.chain.reset();
   SPB_CUDA(cudaDeviceSynchronize());
   mark("work items (host) + upload");
 }

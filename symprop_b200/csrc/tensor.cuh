@@ -57,6 +57,8 @@ struct RowBands {
   std::vector<uint32_t> row0, chunk0, split0;
   DBuf<Chunk> chunks;
   DBuf<SplitRow> split;
+  std::vector<uint32_t> light0;  // chain schedule: the light rows of band k are
+  DBuf<Chunk> light;             // light[light0[k], light0[k+1])
 };
 
 // The work items of one S3TTMc pass: all of them, or one row band.  After the
@@ -67,6 +69,10 @@ struct ItemSet {
   const SplitRow *split = nullptr;
   uint32_t nsplit = 0;
   uint32_t row0 = 0, rows = 0;
+  bool chain = false;      // items of the pivot-chain schedule (ChainData)
+  uint32_t nslots = 0;     // partial-sum slots of the item list
+  const Chunk *light = nullptr;  // chain schedule: light rows, one chunk each
+  uint32_t nlight = 0;
 };
 
 // Reference CompressedDTree arrays, built on demand (tree.cu).
@@ -87,11 +93,12 @@ struct TreeLevels {
 struct PackedTables;
 struct TiledPlan;
 struct WarpPlan;
+struct ChainData;
 
-// S3TTMc schedule: 0 = automatic (warp, else tiled, else rows), 1 = per-owner
-// rows kernel, 2 = CTA register-tiled, 3 = warp per owner (2 and 3 fail on
-// shapes they do not support).
-enum { kScheduleAuto = 0, kScheduleRows = 1, kScheduleTiled = 2, kScheduleWarp = 3 };
+// S3TTMc schedule: 0 = automatic (chain, else warp, else tiled, else rows),
+// 1 = per-owner rows kernel, 2 = CTA register-tiled, 3 = warp per owner,
+// 4 = pivot chain (2, 3 and 4 fail on shapes they do not support).
+enum { kScheduleAuto = 0, kScheduleRows = 1, kScheduleTiled = 2, kScheduleWarp = 3, kScheduleChain = 4 };
 int s3ttmc_schedule();
 void set_s3ttmc_schedule(int s);
 
@@ -128,6 +135,7 @@ struct TensorState {
   std::map<uint32_t, std::shared_ptr<WarpPlan>> warp;        // by R
   std::unique_ptr<TreeLevels> tree;
   std::map<uint32_t, std::unique_ptr<RowBands>> bands;  // by band count
+  std::shared_ptr<ChainData> chain;  // owners in pivot-chain order (s3ttmc_chain.cu)
 };
 
 // s3ttmc.cu
@@ -144,6 +152,12 @@ void tree_build(TensorState &t);
 // tensor.cu
 // inds/vals in host memory, or in device memory when on_device is set
 void tensor_build(TensorState &t, const uint32_t *inds, const double *vals, bool on_device = false);
+// work items over owner ranges [row_ptr[i], row_ptr[i+1]): one per row,
+// rows above co owners cut into slices with partial-sum slots (returns the
+// slot count); and their heaviest-first order
+uint32_t cut_rows(const std::vector<uint64_t> &row_ptr, uint32_t dim, uint64_t co, std::vector<Chunk> &ch,
+                  std::vector<SplitRow> &sp);
+void sort_heaviest_first(std::vector<Chunk> &ch, size_t b, size_t e, uint64_t max_owners);
 // p[i] = i, i < n (permutation seeds of the radix sorts)
 void device_iota(uint32_t *p, uint64_t n, cudaStream_t stream);
 // the work items in nb row bands (built on first use, kept for later calls)

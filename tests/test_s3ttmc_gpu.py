@@ -37,7 +37,7 @@ def test_golden_outputs_fp64_and_fp32(gpu):
         assert rel(Y32.astype(np.float64), g[f"c{ci}_Yp"]) < FP32_TOL, (ci, rel(Y32, g[f"c{ci}_Yp"]))
 
 
-@pytest.fixture(params=[1, 2, 3], ids=["rows", "tiled", "warp"])
+@pytest.fixture(params=[1, 2, 3, 4], ids=["rows", "tiled", "warp", "chain"])
 def schedule(request, gpu):
     assert gpu.lib().symprop_s3ttmc_schedule(request.param) == 0
     yield request.param
@@ -45,11 +45,11 @@ def schedule(request, gpu):
 
 
 def run_or_skip(gpu, schedule, fn):
-    """Schedules 2 and 3 reject shapes they do not cover with ERR_SIZE."""
+    """Schedules 2, 3 and 4 reject shapes they do not cover with ERR_SIZE."""
     try:
         return fn()
     except gpu.SympropError as e:
-        if schedule in (2, 3) and e.status == gpu.ERR_SIZE:
+        if schedule in (2, 3, 4) and e.status == gpu.ERR_SIZE:
             pytest.skip("shape not covered by this schedule")
         raise
 
