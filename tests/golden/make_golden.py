@@ -12,8 +12,11 @@ Fixtures (all small):
                 tensors and factor matrices, orders 3..6
   tucker.json   the reference's per-iteration error lines of HOOI / HOQRI /
                 AltHOOI (symtucker CLI) on seeded tensors, and on the shipped
-                examples/contact-5.tns when present (numbers only; the input
-                file itself is not copied)
+                examples/contact-5.tns when present
+  contact5.npz  the tensor of examples/contact-5.tns as the reference's
+                SymtensLoader reads it (ids sorted within each tuple, values),
+                so that the contact-5 runs can be repeated without the
+                reference tree (python tests/golden/make_golden.py contact5)
   ttmc.npz      the reference's examples/symtens_ttmc driver run on seeded
                 .tns files: the input text, the driver's ttmc.out bytes
 """
@@ -34,7 +37,9 @@ OUT = os.path.dirname(os.path.abspath(__file__))
 PROBE = os.path.join(ROOT, "oracle", "_ref", "ref_probe")
 CLI = os.path.join(ROOT, "oracle", "_ref", "symtucker")
 TTMC = os.path.join(ROOT, "oracle", "_ref", "symtens_ttmc")
-CONTACT5 = "/root/reference/examples/contact-5.tns"
+# the reference tree (SYMPROP_REF, as in oracle/Makefile's REF)
+REF = os.environ.get("SYMPROP_REF", "/root/reference")
+CONTACT5 = os.path.join(REF, "examples", "contact-5.tns")
 
 TREE_CASES = [  # order, n, nnz, seed
     (2, 10, 30, 11), (3, 20, 50, 1), (4, 30, 300, 2), (5, 15, 200, 3), (6, 12, 150, 4), (4, 6, 40, 5),
@@ -114,11 +119,26 @@ def make_ttmc(tmp):
     np.savez_compressed(os.path.join(OUT, "ttmc.npz"), **out)
 
 
+def make_contact5(tmp):
+    """contact-5 as the reference loader reads it (ref_probe load)."""
+    dump = os.path.join(tmp, "contact5.bin")
+    subprocess.run([PROBE, "load", CONTACT5, dump], check=True, capture_output=True)
+    raw = open(dump, "rb").read()
+    order, dim = np.frombuffer(raw[:8], np.uint32)
+    nnz = int(np.frombuffer(raw[8:16], np.uint64)[0])
+    inds = np.frombuffer(raw[16:16 + 4 * nnz * order], np.uint32).reshape(nnz, order)
+    vals = np.frombuffer(raw[16 + 4 * nnz * order:16 + 4 * nnz * order + 8 * nnz], np.float64)
+    np.savez_compressed(os.path.join(OUT, "contact5.npz"), order=np.int64(order), dim=np.int64(dim),
+                        inds=inds.astype(np.uint8 if dim < 256 else np.uint32), vals=vals)
+
+
 def main():
     tmp = tempfile.mkdtemp()
-    want = set(sys.argv[1:]) or {"trees", "s3ttmc", "tucker", "ttmc"}
+    want = set(sys.argv[1:]) or {"trees", "s3ttmc", "tucker", "ttmc", "contact5"}
     if "ttmc" in want:
         make_ttmc(tmp)
+    if "contact5" in want and os.path.exists(CONTACT5):
+        make_contact5(tmp)
     if not want & {"trees", "s3ttmc", "tucker"}:
         print("wrote", os.listdir(OUT))
         return
