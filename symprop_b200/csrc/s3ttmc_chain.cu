@@ -286,6 +286,230 @@ __global__ void __launch_bounds__(kThreads, 4) s3ttmc_chain_kernel(const ChainPa
   }
 }
 
+// ----------------------------------------------------- order 5 (L = 4)
+//
+// Leaf S = {s_1, s_2, s_3, s_4} in pivot order.  With the owners of a row
+// sorted by (s_1, s_2):
+//   T3_h = sum over the owners of h = (s_1, s_2) of c * K({s_3, s_4})  (order 2, m2)
+//   T2_g = sum over the h of g = s_1 of Sym3(U[s_2], T3_h)             (order 3, m3)
+//   G    = sum_g U[s_1] (x) T2_g                                        (16 x m3)
+//   Y    = Sym4(G),  Sym4(G)[q0..q3] = sum_t G[q_t][q without q_t]
+// with Sym3(u, T)[q0 q1 q2] = u[q0] T[q1 q2] + u[q1] T[q0 q2] + u[q2] T[q0 q1].
+// On the order-5 power-law workload a row has 0.19 distinct s_1 and 0.63
+// distinct (s_1, s_2) per owner: about 272 + 0.63 * 2448 + 0.19 * 13056
+// FMAs per owner, against about 39,000 for the leaf-by-leaf team kernel.
+// One CTA of 256 threads per work item; batches of up to kB5 owners, kH5
+// (s_1, s_2) prefixes and kG5 s_1 groups.  Each thread keeps 4 x 13 entries
+// of G (rows 4a..4a+3, columns b + 64 k).
+constexpr int kThreads5 = 256;
+constexpr int kB5 = 128, kH5 = 32, kG5 = 8;
+constexpr int kM3 = 816;                // packed order-3 entries at R = 16
+constexpr int kBeta5 = (kM3 + 63) / 64;  // 13
+
+struct Chain5Params {
+  const Chunk *chunks;
+  uint32_t nchunks;
+  const uint32_t *S;  // nown x 4 leaf ids in pivot order
+  const void *c;
+  const uint8_t *flags;
+  const void *U;
+  uint32_t R, m2, m3, m4;
+  void *Y;            // packed rows, row stride m4
+  double *partials;   // nslots x m4
+  const uint2 *tri;   // m3: q0 | q1 << 8 | q2 << 16 ; p12 | p02 << 8 | p01 << 16 (order-2 indices)
+  const uint4 *quad;  // m4: q0 | q1 << 8 | q2 << 16 | q3 << 24 ; idx3 of q\q0, q\q1 ; q\q2, q\q3 (16 bits each)
+  uint64_t nown;
+  uint32_t nrows, nslots;
+};
+
+template <typename T> struct Smem5 {
+  uint32_t s1[kB5], s2[kB5], s3[kB5], s4[kB5];
+  T c[kB5];
+  uint16_t h_start[kH5 + 1], g_h[kG5 + 1];
+  uint32_t warp_tot[kThreads5 / 32];
+  int nb, nh, ng;
+  uint8_t px[kM2], py[kM2];
+  uint2 tri[kM3];
+  union {
+    struct {
+      T U3[kB5][kRP], U4[kB5][kRP];  // the owners' s_3 and s_4 rows
+      T T3[kH5][kM2];
+      T U2[kH5][kRP];
+      T T2[kG5][kM3];
+      T U1[kG5][kRP];
+    } b;
+    T G[kRP * kM3];                  // the row's G at the end
+  } u;
+};
+
+template <typename T>
+__global__ void __launch_bounds__(kThreads5, (sizeof(T) == 8 ? 1 : 2)) s3ttmc_chain5_kernel(const Chain5Params p) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Smem5<T> &sm = *reinterpret_cast<Smem5<T> *>(smem_raw);
+  const int tid = threadIdx.x;
+  const Chunk ch = p.chunks[blockIdx.x];
+  if (!SPB_BOUND(ch.ob <= ch.oe && ch.oe <= p.nown && ch.row < p.nrows && (ch.slot == kDirect || ch.slot < p.nslots),
+                 211, blockIdx.x))
+    return;
+  const T *U = reinterpret_cast<const T *>(p.U);
+  const T *cc = reinterpret_cast<const T *>(p.c);
+  const uint32_t R = p.R, m2 = p.m2, m3 = p.m3;
+  for (uint32_t b = tid; b < m2; b += kThreads5) {
+    uint32_t x = 0, rem = b;
+    while (rem >= R - x) {
+      rem -= R - x;
+      ++x;
+    }
+    sm.px[b] = (uint8_t)x;
+    sm.py[b] = (uint8_t)(x + rem);
+  }
+  for (uint32_t e = tid; e < m3; e += kThreads5) sm.tri[e] = p.tri[e];
+
+  // this thread's entries of G: rows a4 .. a4 + 3, columns bg + 64 k
+  const int a4 = 4 * (tid & 3), bg = tid >> 2;
+  T gsum[4][kBeta5];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int k = 0; k < kBeta5; ++k) gsum[a][k] = T(0);
+
+  // owner record of window slot tid (tid < kB5), prefetched a batch ahead
+  uint4 rid = make_uint4(0, 0, 0, 0);
+  T rc = T(0);
+  uint32_t rf = 0;
+  auto fetch = [&](uint64_t w0) {
+    const uint64_t o = w0 + (uint64_t)tid;
+    if (tid < kB5 && o < ch.oe) {
+      rid = *reinterpret_cast<const uint4 *>(p.S + o * 4);
+      rc = cc[o];
+      rf = p.flags[o];
+    }
+  };
+  fetch(ch.ob);
+  __syncthreads();
+  for (uint64_t o0 = ch.ob; o0 < ch.oe;) {
+    const uint64_t left = ch.oe - o0;
+    const bool in = tid < kB5 && (uint64_t)tid < left;
+    uint32_t fl = 0;
+    if (in) {
+      uint4 ids = rid;
+      if (!SPB_BOUND(ids.x < p.nrows && ids.y < p.nrows && ids.z < p.nrows && ids.w < p.nrows, 212, o0 + tid))
+        ids = make_uint4(0, 0, 0, 0);
+      sm.s1[tid] = ids.x;
+      sm.s2[tid] = ids.y;
+      sm.s3[tid] = ids.z;
+      sm.s4[tid] = ids.w;
+      sm.c[tid] = rc;
+      const uint32_t f = tid == 0 ? 3u : rf;  // a batch starts a group and a prefix
+      fl = (f & 1u) | (((f >> 1) & 1u) << 16);
+    }
+    const uint32_t cnt = cta_scan(fl, sm.warp_tot);  // inclusive: groups | prefixes << 16
+    auto within = [](uint32_t c) { return (c & 0xffffu) <= (uint32_t)kG5 && (c >> 16) <= (uint32_t)kH5; };
+    const bool v = in && within(cnt);
+    const bool prev_valid = tid > 0 && tid <= kB5 && (uint64_t)(tid - 1) < left && within(cnt - fl);
+    if (!v && prev_valid) sm.nb = tid;
+    if (v && tid == kB5 - 1) sm.nb = kB5;
+    __syncthreads();
+    const int nb = sm.nb;
+    if (v) {
+      const uint32_t g = cnt & 0xffffu, h = cnt >> 16;
+      if (fl >> 16) sm.h_start[h - 1] = (uint16_t)tid;
+      if (fl & 0xffffu) sm.g_h[g - 1] = (uint16_t)(h - 1);
+      if (tid == nb - 1) {
+        sm.nh = (int)h;
+        sm.ng = (int)g;
+        sm.h_start[h] = (uint16_t)nb;
+        sm.g_h[g] = (uint16_t)h;
+      }
+    }
+    __syncthreads();
+    fetch(o0 + (uint64_t)nb);  // in flight during this batch
+    const int nh = sm.nh, ng = sm.ng;
+    // ---- stage the owners' s_3 / s_4 rows and the pivots' s_2 / s_1 rows
+    for (int e = tid; e < nb * kRP; e += kThreads5) {
+      const int i = e / kRP, x = e - i * kRP;
+      sm.u.b.U3[i][x] = (uint32_t)x < R ? U[(uint64_t)sm.s3[i] * R + x] : T(0);
+      sm.u.b.U4[i][x] = (uint32_t)x < R ? U[(uint64_t)sm.s4[i] * R + x] : T(0);
+    }
+    for (int e = tid; e < nh * kRP; e += kThreads5) {
+      const int h = e / kRP, x = e - h * kRP;
+      sm.u.b.U2[h][x] = (uint32_t)x < R ? U[(uint64_t)sm.s2[sm.h_start[h]] * R + x] : T(0);
+    }
+    for (int e = tid; e < ng * kRP; e += kThreads5) {
+      const int g = e / kRP, x = e - g * kRP;
+      sm.u.b.U1[g][x] = (uint32_t)x < R ? U[(uint64_t)sm.s1[sm.h_start[sm.g_h[g]]] * R + x] : T(0);
+    }
+    __syncthreads();
+    // ---- T3 of every prefix h: one thread per (h, x), the row x of T3
+    for (int e = tid; e < nh * kRP; e += kThreads5) {
+      const int h = e / kRP, x = e - h * kRP;
+      if ((uint32_t)x >= R) continue;
+      T acc[kRP];
+#pragma unroll
+      for (int y = 0; y < kRP; ++y) acc[y] = T(0);
+      for (int i = sm.h_start[h]; i < sm.h_start[h + 1]; ++i) {
+        const T c = sm.c[i], a3 = c * sm.u.b.U3[i][x], a4 = c * sm.u.b.U4[i][x];
+#pragma unroll
+        for (int y = 0; y < kRP; ++y) acc[y] += a3 * sm.u.b.U4[i][y] + a4 * sm.u.b.U3[i][y];
+      }
+      // row x of the packed order-2 tensor: entries (x, y), y >= x
+      const uint32_t base = (uint32_t)x * R - ((uint32_t)x * (uint32_t)(x - 1)) / 2;
+#pragma unroll
+      for (int y = 0; y < kRP; ++y)
+        if (y >= x && (uint32_t)y < R) sm.u.b.T3[h][base + (uint32_t)(y - x)] = acc[y];
+    }
+    __syncthreads();
+    // ---- T2 of every group g: Sym3(U2_h, T3_h) over its prefixes
+    for (int e = tid; e < ng * (int)m3; e += kThreads5) {
+      const int g = e / (int)m3, b = e - g * (int)m3;
+      const uint2 tt = sm.tri[b];
+      const uint32_t q0 = tt.x & 0xffu, q1 = (tt.x >> 8) & 0xffu, q2 = (tt.x >> 16) & 0xffu;
+      const uint32_t p12 = tt.y & 0xffu, p02 = (tt.y >> 8) & 0xffu, p01 = (tt.y >> 16) & 0xffu;
+      T acc = T(0);
+      for (int h = sm.g_h[g]; h < sm.g_h[g + 1]; ++h)
+        acc += sm.u.b.U2[h][q0] * sm.u.b.T3[h][p12] + sm.u.b.U2[h][q1] * sm.u.b.T3[h][p02] +
+               sm.u.b.U2[h][q2] * sm.u.b.T3[h][p01];
+      sm.u.b.T2[g][b] = acc;
+    }
+    __syncthreads();
+    // ---- G += U1_g (x) T2_g over the batch's groups
+    for (int g = 0; g < ng; ++g) {
+      T u[4];
+#pragma unroll
+      for (int a = 0; a < 4; ++a) u[a] = sm.u.b.U1[g][a4 + a];
+#pragma unroll
+      for (int k = 0; k < kBeta5; ++k) {
+        const int b = bg + 64 * k;
+        const T t2 = b < (int)m3 ? sm.u.b.T2[g][b] : T(0);
+#pragma unroll
+        for (int a = 0; a < 4; ++a) gsum[a][k] += u[a] * t2;
+      }
+    }
+    o0 += (uint64_t)nb;
+    __syncthreads();
+  }
+  // ---- Y = Sym4(G) through shared memory
+  T *sG = sm.u.G;  // kRP x kM3
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int k = 0; k < kBeta5; ++k) {
+      const int b = bg + 64 * k;
+      if (b < kM3) sG[(a4 + a) * kM3 + b] = gsum[a][k];
+    }
+  __syncthreads();
+  T *Yrow = reinterpret_cast<T *>(p.Y) + (uint64_t)ch.row * p.m4;
+  double *Prow = p.partials + (uint64_t)ch.slot * p.m4;
+  for (uint32_t e = tid; e < p.m4; e += kThreads5) {
+    const uint4 qd = p.quad[e];
+    const uint32_t q0 = qd.x & 0xffu, q1 = (qd.x >> 8) & 0xffu, q2 = (qd.x >> 16) & 0xffu, q3 = qd.x >> 24;
+    const double y = (double)sG[q0 * kM3 + (qd.y & 0xffffu)] + (double)sG[q1 * kM3 + (qd.y >> 16)] +
+                     (double)sG[q2 * kM3 + (qd.z & 0xffffu)] + (double)sG[q3 * kM3 + (qd.z >> 16)];
+    if (ch.slot == kDirect) Yrow[e] = (T)y;
+    else Prow[e] = y;
+  }
+}
+
 // ---------------------------------------------------------------- build
 
 __global__ void degree_kernel(const uint32_t *inds0, uint64_t n, uint32_t *deg) {
@@ -378,6 +602,10 @@ __global__ void chain_flags_kernel(const uint32_t *S, const uint32_t *row_sorted
 
 inline unsigned blocks_for(uint64_t n, unsigned b) { return (unsigned)std::max<uint64_t>(1, (n + b - 1) / b); }
 
+}  // namespace
+uint64_t chain_light_max(const TensorState &t);
+namespace {
+
 template <class V> void upload(DBuf<V> &d, const std::vector<V> &h) {
   d.alloc(h.size());
   if (!h.empty()) SPB_CUDA(cudaMemcpy(d.p, h.data(), h.size() * sizeof(V), cudaMemcpyHostToDevice));
@@ -387,12 +615,12 @@ uint64_t heavy_owner_count(const TensorState &t) {
   uint64_t s = 0;
   for (uint32_t i = 0; i < t.dim; ++i) {
     const uint64_t c = t.h_row_ptr[i + 1] - t.h_row_ptr[i];
-    if (c > kChainLight) s += c;
+    if (c > chain_light_max(t)) s += c;
   }
   return s;
 }
 
-// Items of rows [r0, r1) in row order: rows of at most kChainLight owners
+// Items of rows [r0, r1) in row order: rows of at most chain_light_max owners
 // as one light item each, heavier rows as chain items of at most co owners
 // (a row of several items gets partial-sum slots).  Returns the slot count.
 uint32_t cut_chain_rows(const TensorState &t, uint64_t co, uint32_t r0, uint32_t r1, std::vector<Chunk> &ch,
@@ -403,7 +631,7 @@ uint32_t cut_chain_rows(const TensorState &t, uint64_t co, uint32_t r0, uint32_t
   uint32_t slot = 0;
   for (uint32_t i = r0; i < r1; ++i) {
     const uint64_t b = t.h_row_ptr[i], e = t.h_row_ptr[(size_t)i + 1];
-    if (e - b <= kChainLight) {
+    if (e - b <= chain_light_max(t)) {
       lt.push_back(Chunk{i, kDirect, b, e});
     } else if (e - b <= co) {
       ch.push_back(Chunk{i, kDirect, b, e});
@@ -419,8 +647,11 @@ uint32_t cut_chain_rows(const TensorState &t, uint64_t co, uint32_t r0, uint32_t
 }  // namespace
 
 bool chain_supported(const TensorState &t, uint32_t R) {
-  return t.order == 4 && R >= 1 && R <= (uint32_t)kRP && t.dim < (1u << 24) && t.nown < (1ull << 32);
+  return (t.order == 4 || t.order == 5) && R >= 1 && R <= (uint32_t)kRP && t.dim < (1u << 21) &&
+         t.nown < (1ull << 32);
 }
+
+uint64_t chain_light_max(const TensorState &t) { return t.order == 4 ? kChainLight : 0; }
 
 ChainData &chain_data(TensorState &t) {
   if (t.chain) return *t.chain;
@@ -571,10 +802,94 @@ const uint32_t *triples(uint32_t R) {
 }
 }  // namespace
 
+namespace {
+// Order-5 index tables of rank R (kept per device and R): tri[e] for the
+// packed order-3 entry e = (q0 <= q1 <= q2): the q's and the packed order-2
+// indices of (q1 q2), (q0 q2), (q0 q1); quad[e] for the packed order-4 entry
+// (q0 <= .. <= q3): the q's and the packed order-3 indices of the four
+// triples that leave one q out.
+struct Order5Tables {
+  uint2 *tri = nullptr;
+  uint4 *quad = nullptr;
+};
+
+const Order5Tables &order5_tables(uint32_t R) {
+  static std::mutex mu;
+  static std::map<std::pair<int, uint32_t>, Order5Tables> cache;  // kept for the process
+  int dev = 0;
+  SPB_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(mu);
+  Order5Tables &tb = cache[{dev, R}];
+  if (tb.tri) return tb;
+  std::vector<int> pidx(R * R, -1), tidx(R * R * R, -1);
+  for_each_sorted(R, 2, [&](const std::vector<uint32_t> &q, uint64_t lin) { pidx[q[0] * R + q[1]] = (int)lin; });
+  for_each_sorted(R, 3, [&](const std::vector<uint32_t> &q, uint64_t lin) {
+    tidx[(q[0] * R + q[1]) * R + q[2]] = (int)lin;
+  });
+  auto P = [&](uint32_t a, uint32_t b) { return (uint32_t)pidx[a * R + b]; };
+  auto Tr = [&](uint32_t a, uint32_t b, uint32_t c) { return (uint32_t)tidx[(a * R + b) * R + c]; };
+  std::vector<uint2> tri;
+  for_each_sorted(R, 3, [&](const std::vector<uint32_t> &q, uint64_t) {
+    tri.push_back(make_uint2(q[0] | q[1] << 8 | q[2] << 16, P(q[1], q[2]) | P(q[0], q[2]) << 8 | P(q[0], q[1]) << 16));
+  });
+  std::vector<uint4> quad;
+  for_each_sorted(R, 4, [&](const std::vector<uint32_t> &q, uint64_t) {
+    quad.push_back(make_uint4(q[0] | q[1] << 8 | q[2] << 16 | q[3] << 24,
+                              Tr(q[1], q[2], q[3]) | Tr(q[0], q[2], q[3]) << 16,
+                              Tr(q[0], q[1], q[3]) | Tr(q[0], q[1], q[2]) << 16, 0u));
+  });
+  SPB_CUDA(cudaMalloc(&tb.tri, tri.size() * sizeof(uint2)));
+  SPB_CUDA(cudaMemcpy(tb.tri, tri.data(), tri.size() * sizeof(uint2), cudaMemcpyHostToDevice));
+  SPB_CUDA(cudaMalloc(&tb.quad, quad.size() * sizeof(uint4)));
+  SPB_CUDA(cudaMemcpy(tb.quad, quad.data(), quad.size() * sizeof(uint4), cudaMemcpyHostToDevice));
+  return tb;
+}
+
+void chain5_launch(const TensorState &t, const ChainData &cd, const ItemSet &items, const void *dU, uint32_t R,
+                   void *dYpacked, int precision, cudaStream_t st) {
+  const Order5Tables &tb = order5_tables(R);
+  Chain5Params p;
+  p.chunks = items.chunks;
+  p.nchunks = items.nchunks;
+  p.S = cd.S.p;
+  p.c = precision == SYMPROP_FP64 ? (const void *)cd.c64.p : (const void *)cd.c32.p;
+  p.flags = cd.flags.p;
+  p.U = dU;
+  p.R = R;
+  p.m2 = R * (R + 1) / 2;
+  p.m3 = (uint32_t)symsize(R, 3);
+  p.m4 = (uint32_t)symsize(R, 4);
+  p.Y = dYpacked;
+  p.partials = t.partials.p;
+  p.tri = tb.tri;
+  p.quad = tb.quad;
+  p.nown = t.nown;
+  p.nrows = t.dim;
+  p.nslots = cd.nslots;
+  if (precision == SYMPROP_FP64) {
+    const size_t smem = sizeof(Smem5<double>);
+    SPB_CUDA(cudaFuncSetAttribute(s3ttmc_chain5_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)smem));
+    s3ttmc_chain5_kernel<double><<<items.nchunks, kThreads5, smem, st>>>(p);
+  } else {
+    const size_t smem = sizeof(Smem5<float>);
+    SPB_CUDA(cudaFuncSetAttribute(s3ttmc_chain5_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)smem));
+    s3ttmc_chain5_kernel<float><<<items.nchunks, kThreads5, smem, st>>>(p);
+  }
+  SPB_LAUNCH_CHECK();
+  spb_check_host(st, "S3TTMc chain kernel (order 5)");
+}
+}  // namespace
+
 void chain_launch(const TensorState &t, const ChainData &cd, const ItemSet &items, const void *dU, uint32_t R,
                   void *dYpacked, int precision, cudaStream_t st) {
   if (!chain_supported(t, R)) fail(SYMPROP_ERR_SIZE, "chain S3TTMc does not support order %u rank %u", t.order, R);
   if (!items.nchunks) return;
+  if (t.order == 5) {
+    chain5_launch(t, cd, items, dU, R, dYpacked, precision, st);
+    return;
+  }
   ChainParams p;
   p.chunks = items.chunks;
   p.nchunks = items.nchunks;

@@ -21,9 +21,11 @@ struct ChainData {
   std::map<uint32_t, std::unique_ptr<RowBands>> bands;  // by band count
 };
 
-// Rows with at most this many owners share few pivots; the chain schedule
-// hands them to the warp-per-row kernel.
+// Order 4: rows with at most this many owners share few pivots; the chain
+// schedule hands them to the warp-per-row kernel.  Order 5 keeps every row
+// (the team kernel costs about 9x the chain's FMAs per owner).
 constexpr uint64_t kChainLight = 64;
+uint64_t chain_light_max(const TensorState &t);
 
 // Whether the chain schedule covers this tensor and rank.
 bool chain_supported(const TensorState &t, uint32_t R);
