@@ -77,7 +77,7 @@ template <typename T> struct Smem {
   uint32_t sg_s2[kSG], g_s1[kG];
   uint32_t warp_tot[kThreads / 32];
   int nb, nsg, ng;
-  union {
+  union __align__(16) {
     struct {
       T W[kSG][kRP], U2[kSG][kRP];
       T Q[kG][kM2];
@@ -86,6 +86,21 @@ template <typename T> struct Smem {
     double G[kRP * kM2];        // the row's G at the end (FP64)
   } u;
 };
+
+// Four consecutive values from shared memory (16-byte aligned).
+__device__ __forceinline__ void load4(const double *p, double (&v)[4]) {
+  const double2 a = reinterpret_cast<const double2 *>(p)[0], b = reinterpret_cast<const double2 *>(p)[1];
+  v[0] = a.x, v[1] = a.y, v[2] = b.x, v[3] = b.y;
+}
+__device__ __forceinline__ void load4(const float *p, float (&v)[4]) {
+  const float4 a = *reinterpret_cast<const float4 *>(p);
+  v[0] = a.x, v[1] = a.y, v[2] = a.z, v[3] = a.w;
+}
+
+// Pull the 128-byte line holding a row of U into L1 ahead of its gather.
+__device__ __forceinline__ void prefetch_l1(const void *p) {
+  asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
+}
 
 // Inclusive scan over the CTA of 32-bit values (two 16-bit counts packed).
 __device__ __forceinline__ uint32_t cta_scan(uint32_t v, uint32_t *warp_tot) {
@@ -174,6 +189,10 @@ __global__ void __launch_bounds__(kThreads, 4) s3ttmc_chain_kernel(const ChainPa
         uint32_t f = rec[h].f;
         if (i == 0) f = 3u;  // a batch starts a group and a subgroup
         fl[h] = (f & 1u) | (((f >> 1) & 1u) << 16);
+        // the W / U2 / U1 stages gather these rows after two barriers
+        prefetch_l1(U + (uint64_t)ids.z * R);
+        if (f & 2u) prefetch_l1(U + (uint64_t)ids.y * R);
+        if (f & 1u) prefetch_l1(U + (uint64_t)ids.x * R);
       }
     }
     const uint32_t c1 = cta_scan(fl[0] + fl[1], sm.warp_tot);  // counts through owner 2t+1
@@ -230,17 +249,61 @@ __global__ void __launch_bounds__(kThreads, 4) s3ttmc_chain_kernel(const ChainPa
         sm.u.b.U1[g][x] = (uint32_t)x < R ? U[(uint64_t)sm.g_s1[g] * R + x] : T(0);
     }
     __syncthreads();
-    // ---- Q of every group: sum over its subgroups of U2 (x)s W
-    for (int e = tid; e < ng * (int)m2; e += kThreads) {
-      const int g = e / (int)m2, b = e - g * (int)m2;
-      const uint32_t x = sm.px[b], y = sm.py[b];
-      T q = T(0);
-      for (int sg = sm.g_sg[g]; sg < sm.g_sg[g + 1]; ++sg) q += sm.u.b.U2[sg][x] * sm.u.b.W[sg][y] + sm.u.b.W[sg][x] * sm.u.b.U2[sg][y];
-      sm.u.b.Q[g][b] = q;
+    // ---- Q of every group: sum over its subgroups of U2 (x)s W, one 4 x 4
+    // tile of the upper block triangle per task (tiles in column order:
+    // (0,0), (0,1), (1,1), (0,2), ...)
+    {
+      const int nbk = ((int)R + 3) >> 2, ntile = nbk * (nbk + 1) / 2;
+      for (int e = tid; e < ng * ntile; e += kThreads) {
+        const int g = e / ntile;
+        int X = e - g * ntile, Yb = 0;
+        while (X > Yb) {
+          X -= Yb + 1;
+          ++Yb;
+        }
+        T q[4][4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+          for (int j = 0; j < 4; ++j) q[i][j] = T(0);
+        for (int sg = sm.g_sg[g]; sg < sm.g_sg[g + 1]; ++sg) {
+          T ux[4], wx[4], uy[4], wy[4];
+          load4(&sm.u.b.U2[sg][4 * X], ux);
+          load4(&sm.u.b.W[sg][4 * X], wx);
+          load4(&sm.u.b.U2[sg][4 * Yb], uy);
+          load4(&sm.u.b.W[sg][4 * Yb], wy);
+#pragma unroll
+          for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+              q[i][j] = fma(ux[i], wy[j], q[i][j]);
+              q[i][j] = fma(wx[i], uy[j], q[i][j]);
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+          for (int j = 0; j < 4; ++j) {
+            const uint32_t x = 4 * X + i, y = 4 * Yb + j;
+            if (x <= y && y < R) sm.u.b.Q[g][pair_index(x, y, R)] = q[i][j];
+          }
+      }
     }
     __syncthreads();
-    // ---- G += U1 (x) Q over the batch's groups
-    {
+    // ---- G += U1 (x) Q over the batch's groups (FP64: straight into the
+    // row totals; FP32: a batch sum in FP32, folded into the FP64 totals)
+    if constexpr (sizeof(T) == 8) {
+      for (int g = 0; g < ng; ++g) {
+        const double2 u = *reinterpret_cast<const double2 *>(&sm.u.b.U1[g][a0]);
+#pragma unroll
+        for (int k = 0; k < kBeta; ++k) {
+          const int b = b0 + 16 * k;
+          const double q = b < (int)m2 ? (double)sm.u.b.Q[g][b] : 0.0;
+          gsum[0][k] = fma(u.x, q, gsum[0][k]);
+          gsum[1][k] = fma(u.y, q, gsum[1][k]);
+        }
+      }
+    } else {
       T acc[2][kBeta];
 #pragma unroll
       for (int a = 0; a < 2; ++a)
