@@ -75,6 +75,9 @@ template <typename T> struct Smem {
   T c[kB];
   uint16_t sg_start[kSG + 1], g_sg[kG + 1];
   uint32_t sg_s2[kSG], g_s1[kG];
+  uint8_t sg_of[kB];             // subgroup of each owner of the batch
+  T carry[kThreads / 16][kRP];   // W of a subgroup begun in an earlier lane
+  int carry_sg[kThreads / 16];
   uint32_t warp_tot[kThreads / 32];
   int nb, nsg, ng;
   union __align__(16) {
@@ -215,6 +218,7 @@ __global__ void __launch_bounds__(kThreads, 4) s3ttmc_chain_kernel(const ChainPa
       if (!v[h]) continue;
       const int i = 2 * tid + h;
       const uint32_t g = cnt[h] & 0xffffu, sg = cnt[h] >> 16;
+      sm.sg_of[i] = (uint8_t)(sg - 1);
       if (fl[h] >> 16) {
         sm.sg_start[sg - 1] = (uint16_t)i;
         sm.sg_s2[sg - 1] = sm.s2[i];
@@ -232,31 +236,77 @@ __global__ void __launch_bounds__(kThreads, 4) s3ttmc_chain_kernel(const ChainPa
     }
     __syncthreads();
     const int nsg = sm.nsg, ng = sm.ng;
-    // ---- W of every subgroup (and its s_2 row of U)
+    // ---- W of every subgroup.  Lane j (16 threads, one per column)
+    // sums the owners [nb j / 8, nb (j + 1) / 8) in order, whatever the
+    // subgroup sizes; the part of a subgroup begun in an earlier lane goes
+    // to carry[j] and is added after the barrier, lanes in order.
     {
-      const int x = tid & 15;
-      for (int sg = tid >> 4; sg < nsg; sg += kThreads / 16) {
-        T w = T(0), u2 = T(0);
-        if ((uint32_t)x < R) {
-#pragma unroll 4
-          for (int i = sm.sg_start[sg]; i < sm.sg_start[sg + 1]; ++i) w += sm.c[i] * U[(uint64_t)sm.s3[i] * R + x];
-          u2 = U[(uint64_t)sm.sg_s2[sg] * R + x];
+      constexpr int kLanes = kThreads / 16;
+      const int x = tid & 15, j = tid >> 4;
+      const int i0 = nb * j / kLanes, i1 = nb * (j + 1) / kLanes;
+      const bool xin = (uint32_t)x < R;
+      if (x == 0) sm.carry_sg[j] = -1;
+      if (i0 < i1) {
+        int cur = sm.sg_of[i0];
+        bool own = sm.sg_start[cur] == i0;
+        T w = T(0);
+        auto flush = [&]() {
+          if (own) {
+            sm.u.b.W[cur][x] = w;
+          } else {
+            sm.carry[j][x] = w;
+            if (x == 0) sm.carry_sg[j] = cur;
+          }
+        };
+        for (int i = i0; i < i1; i += 4) {
+          T uv[4];
+#pragma unroll
+          for (int k = 0; k < 4; ++k) uv[k] = (i + k < i1 && xin) ? U[(uint64_t)sm.s3[i + k] * R + x] : T(0);
+#pragma unroll
+          for (int k = 0; k < 4; ++k) {
+            if (i + k >= i1) break;
+            const int sg = sm.sg_of[i + k];
+            if (sg != cur) {
+              flush();
+              w = T(0);
+              cur = sg;
+              own = true;
+            }
+            w = fma(sm.c[i + k], uv[k], w);
+          }
         }
-        sm.u.b.W[sg][x] = w;
-        sm.u.b.U2[sg][x] = u2;
+        flush();
       }
-      for (int g = tid >> 4; g < ng; g += kThreads / 16)
-        sm.u.b.U1[g][x] = (uint32_t)x < R ? U[(uint64_t)sm.g_s1[g] * R + x] : T(0);
+      // the s_2 row of every subgroup and the s_1 row of every group
+      for (int e = tid; e < nsg * kRP; e += kThreads) {
+        const int sg = e >> 4, xx = e & 15;
+        sm.u.b.U2[sg][xx] = (uint32_t)xx < R ? U[(uint64_t)sm.sg_s2[sg] * R + xx] : T(0);
+      }
+      for (int e = tid; e < ng * kRP; e += kThreads) {
+        const int g = e >> 4, xx = e & 15;
+        sm.u.b.U1[g][xx] = (uint32_t)xx < R ? U[(uint64_t)sm.g_s1[g] * R + xx] : T(0);
+      }
+      __syncthreads();
+      if (tid < kRP)
+        for (int jj = 1; jj < kLanes; ++jj) {
+          const int sg = sm.carry_sg[jj];
+          if (sg >= 0) sm.u.b.W[sg][tid] += sm.carry[jj][tid];
+        }
     }
     __syncthreads();
     // ---- Q of every group: sum over its subgroups of U2 (x)s W, one 4 x 4
     // tile of the upper block triangle per task (tiles in column order:
-    // (0,0), (0,1), (1,1), (0,2), ...)
+    // (0,0), (0,1), (1,1), (0,2), ...).  A batch of few groups splits each
+    // group's subgroups into P parts (slots g P .. g P + P - 1 of Q), so that
+    // one large group does not leave most threads idle; the parts are added
+    // into slot g P before the G stage.
+    const int P = max(1, min(kG / ng, nsg / (4 * ng)));
     {
       const int nbk = ((int)R + 3) >> 2, ntile = nbk * (nbk + 1) / 2;
-      for (int e = tid; e < ng * ntile; e += kThreads) {
-        const int g = e / ntile;
-        int X = e - g * ntile, Yb = 0;
+      for (int e = tid; e < ng * P * ntile; e += kThreads) {
+        const int gp = e / ntile, g = gp / P, part = gp - g * P;
+        const int s0 = sm.g_sg[g], len = sm.g_sg[g + 1] - s0;
+        int X = e - gp * ntile, Yb = 0;
         while (X > Yb) {
           X -= Yb + 1;
           ++Yb;
@@ -266,7 +316,7 @@ __global__ void __launch_bounds__(kThreads, 4) s3ttmc_chain_kernel(const ChainPa
         for (int i = 0; i < 4; ++i)
 #pragma unroll
           for (int j = 0; j < 4; ++j) q[i][j] = T(0);
-        for (int sg = sm.g_sg[g]; sg < sm.g_sg[g + 1]; ++sg) {
+        for (int sg = s0 + len * part / P; sg < s0 + len * (part + 1) / P; ++sg) {
           T ux[4], wx[4], uy[4], wy[4];
           load4(&sm.u.b.U2[sg][4 * X], ux);
           load4(&sm.u.b.W[sg][4 * X], wx);
@@ -285,11 +335,20 @@ __global__ void __launch_bounds__(kThreads, 4) s3ttmc_chain_kernel(const ChainPa
 #pragma unroll
           for (int j = 0; j < 4; ++j) {
             const uint32_t x = 4 * X + i, y = 4 * Yb + j;
-            if (x <= y && y < R) sm.u.b.Q[g][pair_index(x, y, R)] = q[i][j];
+            if (x <= y && y < R) sm.u.b.Q[gp][pair_index(x, y, R)] = q[i][j];
           }
       }
     }
     __syncthreads();
+    if (P > 1) {
+      for (int e = tid; e < ng * (int)m2; e += kThreads) {
+        const int g = e / (int)m2, b = e - g * (int)m2;
+        T q = sm.u.b.Q[g * P][b];
+        for (int part = 1; part < P; ++part) q += sm.u.b.Q[g * P + part][b];
+        sm.u.b.Q[g * P][b] = q;
+      }
+      __syncthreads();
+    }
     // ---- G += U1 (x) Q over the batch's groups (FP64: straight into the
     // row totals; FP32: a batch sum in FP32, folded into the FP64 totals)
     if constexpr (sizeof(T) == 8) {
@@ -298,7 +357,7 @@ __global__ void __launch_bounds__(kThreads, 4) s3ttmc_chain_kernel(const ChainPa
 #pragma unroll
         for (int k = 0; k < kBeta; ++k) {
           const int b = b0 + 16 * k;
-          const double q = b < (int)m2 ? (double)sm.u.b.Q[g][b] : 0.0;
+          const double q = b < (int)m2 ? (double)sm.u.b.Q[g * P][b] : 0.0;
           gsum[0][k] = fma(u.x, q, gsum[0][k]);
           gsum[1][k] = fma(u.y, q, gsum[1][k]);
         }
@@ -314,7 +373,7 @@ __global__ void __launch_bounds__(kThreads, 4) s3ttmc_chain_kernel(const ChainPa
 #pragma unroll
         for (int k = 0; k < kBeta; ++k) {
           const int b = b0 + 16 * k;
-          const T q = b < (int)m2 ? sm.u.b.Q[g][b] : T(0);
+          const T q = b < (int)m2 ? sm.u.b.Q[g * P][b] : T(0);
           acc[0][k] += u0 * q;
           acc[1][k] += u1 * q;
         }
