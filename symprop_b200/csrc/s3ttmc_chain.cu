@@ -100,6 +100,13 @@ __device__ __forceinline__ void load4(const float *p, float (&v)[4]) {
   v[0] = a.x, v[1] = a.y, v[2] = a.z, v[3] = a.w;
 }
 
+// Asynchronous 16-byte copy global -> shared (both 16-byte aligned).
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+  const uint32_t d = (uint32_t)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 // Pull the 128-byte line holding a row of U into L1 ahead of its gather.
 __device__ __forceinline__ void prefetch_l1(const void *p) {
   asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
@@ -438,7 +445,7 @@ struct Chain5Params {
   uint32_t R, m2, m3, m4;
   void *Y;            // packed rows, row stride m4
   double *partials;   // nslots x m4
-  const uint2 *tri;   // m3: q0 | q1 << 8 | q2 << 16 ; p12 | p02 << 8 | p01 << 16 (order-2 indices)
+  const uint2 *tri;   // m3: offsets in F of the three terms of Sym3 (o0 | o1 << 16 ; o2)
   const uint4 *quad;  // m4: q0 | q1 << 8 | q2 << 16 | q3 << 24 ; idx3 of q\q0, q\q1 ; q\q2, q\q3 (16 bits each)
   uint64_t nown;
   uint32_t nrows, nslots;
@@ -452,13 +459,14 @@ template <typename T> struct Smem5 {
   int nb, nh, ng;
   uint8_t px[kM2], py[kM2];
   uint2 tri[kM3];
-  union {
+  union __align__(16) {
     struct {
       T U3[kB5][kRP], U4[kB5][kRP];  // the owners' s_3 and s_4 rows
       T T3[kH5][kM2];
       T U2[kH5][kRP];
       T T2[kG5][kM3];
       T U1[kG5][kRP];
+      T F[2][kRP * kM2];             // F of a group (two buffers)
     } b;
     T G[kRP * kM3];                  // the row's G at the end
   } u;
@@ -476,6 +484,7 @@ __global__ void __launch_bounds__(kThreads5, (sizeof(T) == 8 ? 1 : 2)) s3ttmc_ch
   const T *U = reinterpret_cast<const T *>(p.U);
   const T *cc = reinterpret_cast<const T *>(p.c);
   const uint32_t R = p.R, m2 = p.m2, m3 = p.m3;
+  const bool rows16 = R == (uint32_t)kRP && (reinterpret_cast<uintptr_t>(p.U) & 15u) == 0;
   for (uint32_t b = tid; b < m2; b += kThreads5) {
     uint32_t x = 0, rem = b;
     while (rem >= R - x) {
@@ -547,19 +556,40 @@ __global__ void __launch_bounds__(kThreads5, (sizeof(T) == 8 ? 1 : 2)) s3ttmc_ch
     __syncthreads();
     fetch(o0 + (uint64_t)nb);  // in flight during this batch
     const int nh = sm.nh, ng = sm.ng;
-    // ---- stage the owners' s_3 / s_4 rows and the pivots' s_2 / s_1 rows
-    for (int e = tid; e < nb * kRP; e += kThreads5) {
-      const int i = e / kRP, x = e - i * kRP;
-      sm.u.b.U3[i][x] = (uint32_t)x < R ? U[(uint64_t)sm.s3[i] * R + x] : T(0);
-      sm.u.b.U4[i][x] = (uint32_t)x < R ? U[(uint64_t)sm.s4[i] * R + x] : T(0);
-    }
-    for (int e = tid; e < nh * kRP; e += kThreads5) {
-      const int h = e / kRP, x = e - h * kRP;
-      sm.u.b.U2[h][x] = (uint32_t)x < R ? U[(uint64_t)sm.s2[sm.h_start[h]] * R + x] : T(0);
-    }
-    for (int e = tid; e < ng * kRP; e += kThreads5) {
-      const int g = e / kRP, x = e - g * kRP;
-      sm.u.b.U1[g][x] = (uint32_t)x < R ? U[(uint64_t)sm.s1[sm.h_start[sm.g_h[g]]] * R + x] : T(0);
+    // ---- stage the owners' s_3 / s_4 rows and the pivots' s_2 / s_1 rows;
+    // at R = 16 (rows of whole 16-byte pieces) as asynchronous copies that
+    // are all in flight at once
+    if (rows16) {
+      constexpr int kC = kRP * (int)sizeof(T) / 16;  // 16-byte pieces per row
+      constexpr int kE = 16 / (int)sizeof(T);        // elements per piece
+      for (int e = tid; e < nb * 2 * kC; e += kThreads5) {
+        const int i = e / (2 * kC), r = e - i * 2 * kC, w = r / kC, k = r - w * kC;
+        const uint32_t s = w ? sm.s4[i] : sm.s3[i];
+        cp_async16(w ? &sm.u.b.U4[i][k * kE] : &sm.u.b.U3[i][k * kE], U + (uint64_t)s * kRP + k * kE);
+      }
+      for (int e = tid; e < nh * kC; e += kThreads5) {
+        const int h = e / kC, k = e - h * kC;
+        cp_async16(&sm.u.b.U2[h][k * kE], U + (uint64_t)sm.s2[sm.h_start[h]] * kRP + k * kE);
+      }
+      for (int e = tid; e < ng * kC; e += kThreads5) {
+        const int g = e / kC, k = e - g * kC;
+        cp_async16(&sm.u.b.U1[g][k * kE], U + (uint64_t)sm.s1[sm.h_start[sm.g_h[g]]] * kRP + k * kE);
+      }
+      cp_async_wait_all();
+    } else {
+      for (int e = tid; e < nb * kRP; e += kThreads5) {
+        const int i = e / kRP, x = e - i * kRP;
+        sm.u.b.U3[i][x] = (uint32_t)x < R ? U[(uint64_t)sm.s3[i] * R + x] : T(0);
+        sm.u.b.U4[i][x] = (uint32_t)x < R ? U[(uint64_t)sm.s4[i] * R + x] : T(0);
+      }
+      for (int e = tid; e < nh * kRP; e += kThreads5) {
+        const int h = e / kRP, x = e - h * kRP;
+        sm.u.b.U2[h][x] = (uint32_t)x < R ? U[(uint64_t)sm.s2[sm.h_start[h]] * R + x] : T(0);
+      }
+      for (int e = tid; e < ng * kRP; e += kThreads5) {
+        const int g = e / kRP, x = e - g * kRP;
+        sm.u.b.U1[g][x] = (uint32_t)x < R ? U[(uint64_t)sm.s1[sm.h_start[sm.g_h[g]]] * R + x] : T(0);
+      }
     }
     __syncthreads();
     // ---- T3 of every prefix h: one thread per (h, x), the row x of T3
@@ -581,17 +611,46 @@ __global__ void __launch_bounds__(kThreads5, (sizeof(T) == 8 ? 1 : 2)) s3ttmc_ch
         if (y >= x && (uint32_t)y < R) sm.u.b.T3[h][base + (uint32_t)(y - x)] = acc[y];
     }
     __syncthreads();
-    // ---- T2 of every group g: Sym3(U2_h, T3_h) over its prefixes
-    for (int e = tid; e < ng * (int)m3; e += kThreads5) {
-      const int g = e / (int)m3, b = e - g * (int)m3;
-      const uint2 tt = sm.tri[b];
-      const uint32_t q0 = tt.x & 0xffu, q1 = (tt.x >> 8) & 0xffu, q2 = (tt.x >> 16) & 0xffu;
-      const uint32_t p12 = tt.y & 0xffu, p02 = (tt.y >> 8) & 0xffu, p01 = (tt.y >> 16) & 0xffu;
-      T acc = T(0);
-      for (int h = sm.g_h[g]; h < sm.g_h[g + 1]; ++h)
-        acc += sm.u.b.U2[h][q0] * sm.u.b.T3[h][p12] + sm.u.b.U2[h][q1] * sm.u.b.T3[h][p02] +
-               sm.u.b.U2[h][q2] * sm.u.b.T3[h][p01];
-      sm.u.b.T2[g][b] = acc;
+    // ---- T2 of every group g, one group at a time:
+    //   F_g = sum over its prefixes h of U2_h (x) T3_h    (16 x m2; rows
+    //         r4 .. r4 + 3 and columns c + 64 j of it per thread)
+    //   T2_g[q0 q1 q2] = F_g[q0][q1 q2] + F_g[q1][q0 q2] + F_g[q2][q0 q1]
+    // F alternates between two buffers, so one barrier per group suffices.
+    {
+      const int r4 = 4 * (tid & 3), c0 = tid >> 2;
+      for (int g = 0; g < ng; ++g) {
+        T f[4][3];
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+          for (int j = 0; j < 3; ++j) f[a][j] = T(0);
+        for (int h = sm.g_h[g]; h < sm.g_h[g + 1]; ++h) {
+          T u[4], t[3];
+          load4(&sm.u.b.U2[h][r4], u);
+#pragma unroll
+          for (int j = 0; j < 3; ++j) {
+            const int col = c0 + 64 * j;
+            t[j] = col < (int)m2 ? sm.u.b.T3[h][col] : T(0);
+          }
+#pragma unroll
+          for (int a = 0; a < 4; ++a)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) f[a][j] = fma(u[a], t[j], f[a][j]);
+        }
+        T *F = sm.u.b.F[g & 1];
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+          for (int j = 0; j < 3; ++j) {
+            const int col = c0 + 64 * j;
+            if (col < kM2) F[(r4 + a) * kM2 + col] = f[a][j];
+          }
+        __syncthreads();
+        for (int e = tid; e < (int)m3; e += kThreads5) {
+          const uint2 o = sm.tri[e];
+          sm.u.b.T2[g][e] = F[o.x & 0xffffu] + F[o.x >> 16] + F[o.y];
+        }
+      }
     }
     __syncthreads();
     // ---- G += U1_g (x) T2_g over the batch's groups
@@ -926,8 +985,9 @@ const uint32_t *triples(uint32_t R) {
 
 namespace {
 // Order-5 index tables of rank R (kept per device and R): tri[e] for the
-// packed order-3 entry e = (q0 <= q1 <= q2): the q's and the packed order-2
-// indices of (q1 q2), (q0 q2), (q0 q1); quad[e] for the packed order-4 entry
+// packed order-3 entry e = (q0 <= q1 <= q2): the offsets in the 16 x kM2
+// array F of (q0, (q1 q2)), (q1, (q0 q2)) and (q2, (q0 q1)), order-2
+// entries packed; quad[e] for the packed order-4 entry
 // (q0 <= .. <= q3): the q's and the packed order-3 indices of the four
 // triples that leave one q out.
 struct Order5Tables {
@@ -952,7 +1012,8 @@ const Order5Tables &order5_tables(uint32_t R) {
   auto Tr = [&](uint32_t a, uint32_t b, uint32_t c) { return (uint32_t)tidx[(a * R + b) * R + c]; };
   std::vector<uint2> tri;
   for_each_sorted(R, 3, [&](const std::vector<uint32_t> &q, uint64_t) {
-    tri.push_back(make_uint2(q[0] | q[1] << 8 | q[2] << 16, P(q[1], q[2]) | P(q[0], q[2]) << 8 | P(q[0], q[1]) << 16));
+    const uint32_t o0 = q[0] * kM2 + P(q[1], q[2]), o1 = q[1] * kM2 + P(q[0], q[2]), o2 = q[2] * kM2 + P(q[0], q[1]);
+    tri.push_back(make_uint2(o0 | o1 << 16, o2));
   });
   std::vector<uint4> quad;
   for_each_sorted(R, 4, [&](const std::vector<uint32_t> &q, uint64_t) {
