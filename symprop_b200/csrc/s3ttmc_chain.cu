@@ -265,12 +265,12 @@ __global__ void __launch_bounds__(kThreads, 4) s3ttmc_chain_kernel(const ChainPa
             if (x == 0) sm.carry_sg[j] = cur;
           }
         };
-        for (int i = i0; i < i1; i += 4) {
-          T uv[4];
+        for (int i = i0; i < i1; i += 8) {
+          T uv[8];
 #pragma unroll
-          for (int k = 0; k < 4; ++k) uv[k] = (i + k < i1 && xin) ? U[(uint64_t)sm.s3[i + k] * R + x] : T(0);
+          for (int k = 0; k < 8; ++k) uv[k] = (i + k < i1 && xin) ? U[(uint64_t)sm.s3[i + k] * R + x] : T(0);
 #pragma unroll
-          for (int k = 0; k < 4; ++k) {
+          for (int k = 0; k < 8; ++k) {
             if (i + k >= i1) break;
             const int sg = sm.sg_of[i + k];
             if (sg != cur) {
