@@ -9,9 +9,11 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdint>
 #include <cstdlib>
 #include <map>
 #include <mutex>
+#include <type_traits>
 #include <vector>
 
 #include "dense.cuh"
@@ -91,6 +93,109 @@ __global__ void __launch_bounds__(256) gemm_tile_kernel(int M, int N, int K, con
     for (int j = 0; j < 4; ++j) {
       int gj = bn + tx * 4 + j;
       if (gj < N) o[(size_t)gi * ldo + gj] = acc[i][j];
+    }
+  }
+}
+
+// ------------------------------------------------ FP64 Gram C = A^T A
+//
+// The m x m Gram of the columns of a row-major n x m matrix (HOOI's dense
+// step in FP64), upper tiles only: 128 x 128 tiles of C, 256 threads with
+// 8 x 8 accumulators each (rows ty*4 + {0..3} and 64 + ty*4 + {0..3}, the
+// same for the columns with tx), k-blocks of 16 rows of A staged in shared
+// memory by cp.async in a 3-stage ring.  The K axis is cut into splits
+// whose partial tiles the finalize kernel adds (and mirrors).
+constexpr int GB = 128, GK = 16, GST = 3;
+
+struct GramSmem {
+  double a[GST][GK][GB];
+  double b[GST][GK][GB];
+};
+
+__device__ __forceinline__ void cp_async16_zfill(void *dst, const void *src, bool full) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  const int sz = full ? 16 : 0;  // 0: fill the 16 bytes with zeros, read nothing
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(d), "l"(src), "r"(sz) : "memory");
+}
+
+__global__ void __launch_bounds__(256, 1) gram_tn_f64_kernel(int M, int K, const double *__restrict__ A, int lda,
+                                                             int ntile, int kchunk, double *out,
+                                                             size_t split_stride) {
+  extern __shared__ __align__(16) unsigned char gram_raw[];
+  GramSmem &sm = *reinterpret_cast<GramSmem *>(gram_raw);
+  // upper tile (ti, tj), ti <= tj, of linear index blockIdx.x (row by row)
+  int ti = 0, rem = (int)blockIdx.x;
+  while (rem >= ntile - ti) {
+    rem -= ntile - ti;
+    ++ti;
+  }
+  const int tj = ti + rem;
+  const bool diag = ti == tj;
+  const int i0 = ti * GB, j0 = tj * GB;
+  const int k0 = (int)blockIdx.y * kchunk, k1 = min(K, k0 + kchunk);
+  const int nkb = (k1 - k0 + GK - 1) / GK;
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+
+  auto load = [&](int kb, int stage) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int c = tid + 256 * q, kr = c >> 6, col = (c & 63) * 2;
+      const int gk = k0 + kb * GK + kr;
+      const bool oka = gk < k1 && i0 + col < M;
+      cp_async16_zfill(&sm.a[stage][kr][col], oka ? A + (size_t)gk * lda + i0 + col : A, oka);
+      if (!diag) {
+        const bool okb = gk < k1 && j0 + col < M;
+        cp_async16_zfill(&sm.b[stage][kr][col], okb ? A + (size_t)gk * lda + j0 + col : A, okb);
+      }
+    }
+  };
+#pragma unroll
+  for (int s = 0; s < GST - 1; ++s) {
+    if (s < nkb) load(s, s);
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  }
+  double acc[8][8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int j = 0; j < 8; ++j) acc[i][j] = 0.0;
+  for (int kb = 0; kb < nkb; ++kb) {
+    asm volatile("cp.async.wait_group %0;" ::"n"(GST - 2) : "memory");
+    __syncthreads();
+    if (kb + GST - 1 < nkb) load(kb + GST - 1, (kb + GST - 1) % GST);
+    asm volatile("cp.async.commit_group;" ::: "memory");
+    const int stg = kb % GST;
+    const double(*As)[GB] = sm.a[stg];
+    const double(*Bs)[GB] = diag ? sm.a[stg] : sm.b[stg];
+#pragma unroll 4
+    for (int kk = 0; kk < GK; ++kk) {
+      double a[8], b[8];
+      const double2 a0 = *reinterpret_cast<const double2 *>(&As[kk][ty * 4]);
+      const double2 a1 = *reinterpret_cast<const double2 *>(&As[kk][ty * 4 + 2]);
+      const double2 a2 = *reinterpret_cast<const double2 *>(&As[kk][64 + ty * 4]);
+      const double2 a3 = *reinterpret_cast<const double2 *>(&As[kk][64 + ty * 4 + 2]);
+      const double2 b0 = *reinterpret_cast<const double2 *>(&Bs[kk][tx * 4]);
+      const double2 b1 = *reinterpret_cast<const double2 *>(&Bs[kk][tx * 4 + 2]);
+      const double2 b2 = *reinterpret_cast<const double2 *>(&Bs[kk][64 + tx * 4]);
+      const double2 b3 = *reinterpret_cast<const double2 *>(&Bs[kk][64 + tx * 4 + 2]);
+      a[0] = a0.x, a[1] = a0.y, a[2] = a1.x, a[3] = a1.y, a[4] = a2.x, a[5] = a2.y, a[6] = a3.x, a[7] = a3.y;
+      b[0] = b0.x, b[1] = b0.y, b[2] = b1.x, b[3] = b1.y, b[4] = b2.x, b[5] = b2.y, b[6] = b3.x, b[7] = b3.y;
+#pragma unroll
+      for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+    }
+  }
+  asm volatile("cp.async.wait_group 0;" ::: "memory");
+  double *o = out + blockIdx.y * split_stride;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    const int gi = i0 + (i < 4 ? ty * 4 + i : 64 + ty * 4 + (i - 4));
+    if (gi >= M) continue;
+#pragma unroll
+    for (int jh = 0; jh < 4; ++jh) {
+      const int gj = j0 + (jh < 2 ? tx * 4 + 2 * jh : 64 + tx * 4 + 2 * (jh - 2));
+      if (gj < M) *reinterpret_cast<double2 *>(&o[(size_t)gi * M + gj]) = make_double2(acc[i][2 * jh], acc[i][2 * jh + 1]);
     }
   }
 }
@@ -583,6 +688,39 @@ __global__ void core_reduce_kernel(const double *__restrict__ P, int chunks, int
 
 // ------------------------------------------------------------ public API
 
+// C = A^T A (upper tiles computed, the rest mirrored) for a row-major
+// K x M matrix A; M even, lda even, A 16-byte aligned.
+static void gram_f64(cudaStream_t st, int M, int K, const double *A, int lda, double *C, int ldc) {
+  static int nsm = 0;
+  if (!nsm) {
+    int dev = 0;
+    SPB_CUDA(cudaGetDevice(&dev));
+    SPB_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  }
+  const int nt = (M + GB - 1) / GB;
+  const long long tiles = (long long)nt * (nt + 1) / 2;
+  // the fewest K splits (each at least 1024 rows) that fill 90% of the
+  // waves of one CTA per SM
+  int splits = 1;
+  for (int s = 1; s <= 8; ++s) {
+    if (s > 1 && K / s < 1024) break;
+    const long long ctas = tiles * s, waves = (ctas + nsm - 1) / nsm;
+    splits = s;
+    if ((double)ctas >= 0.9 * (double)(waves * nsm)) break;
+  }
+  const int kchunk = (int)(cdiv(cdiv(K, splits), GK) * GK);
+  splits = std::max(1, (int)cdiv(K, kchunk));
+  Scratch ws(sizeof(double) * (size_t)splits * M * M, st);
+  const size_t smem = sizeof(GramSmem);
+  SPB_CUDA(cudaFuncSetAttribute(gram_tn_f64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  gram_tn_f64_kernel<<<dim3((unsigned)tiles, (unsigned)splits), 256, smem, st>>>(M, K, A, lda, nt, kchunk,
+                                                                                 ws.as<double>(), (size_t)M * M);
+  SPB_LAUNCH_CHECK();
+  gemm_finalize_kernel<double><<<cdiv((long long)M * M, 256), 256, 0, st>>>(M, M, ws.as<double>(), splits,
+                                                                           (size_t)M * M, 1.0, 0.0, C, ldc, 1);
+  SPB_LAUNCH_CHECK();
+}
+
 template <typename T>
 void gemm(cudaStream_t st, int M, int N, int K, T alpha, const T *A, int lda, bool transA,
           const T *B, int ldb, bool transB, T beta, T *C, int ldc, const T *kscale,
@@ -591,6 +729,13 @@ void gemm(cudaStream_t st, int M, int N, int K, T alpha, const T *A, int lda, bo
   if (K <= 0) {
     if (beta == T(0)) {
       for (int i = 0; i < M; ++i) SPB_CUDA(cudaMemsetAsync(C + (size_t)i * ldc, 0, N * sizeof(T), st));
+      return;
+    }
+  }
+  if constexpr (std::is_same<T, double>::value) {
+    if (transA && !transB && sym_upper && A == B && lda == ldb && M == N && !kscale && M >= GB && M % 2 == 0 &&
+        lda % 2 == 0 && (reinterpret_cast<uintptr_t>(A) & 15) == 0 && alpha == 1.0 && beta == 0.0) {
+      gram_f64(st, M, K, A, lda, C, ldc);
       return;
     }
   }
