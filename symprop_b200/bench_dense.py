@@ -7,7 +7,10 @@ its operand, allocates its workspace and synchronises):
   * gram   G = (Y D^1/2)^T (Y D^1/2), m x m, tcgen05 split-BF16
            (symprop_gram_device, FP32 input);
   * panel  W = (Y D^1/2)(V D^1/2)^T, n x r (symprop_symgemm_device);
-  * rows   G = (Y D^1/2)(Y D^1/2)^T for an n <= m slice (symprop_symsyrk_device).
+  * rows   G = (Y D^1/2)(Y D^1/2)^T for an n <= m slice (symprop_symsyrk_device);
+  * gram64 the same m x m Gram from an FP64 Y on the CUDA cores (symprop_gram_device,
+           FP64 input: HOOI's dense step in FP64), against the nominal FP64 rate
+           of a B200 (37 TFLOP/s).
 Rates count the tensor-core work the split needs: three BF16 products over
 the upper-triangular half of a Gram (m (m + 1) / 2 entries, K = n), all
 n r entries of the panel.  Peaks from MEASURED_PEAKS.json when present.
@@ -22,7 +25,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 def main():
     import torch
 
-    from . import gram_device, lib, symgemm_device, symsyrk_device, FP32
+    from . import FP32, FP64, gram_device, lib, symgemm_device, symsyrk_device
     ap = argparse.ArgumentParser()
     ap.add_argument("--n", type=int, default=200000)
     ap.add_argument("--m", type=int, default=3876)
@@ -30,7 +33,7 @@ def main():
     ap.add_argument("--rows", type=int, default=2048, help="rows of the row-Gram case")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--steps", type=int, default=10)
-    ap.add_argument("--only", default="gram,panel,rows")
+    ap.add_argument("--only", default="gram,panel,rows,gram64")
     a = ap.parse_args()
     lib()
     torch.cuda.set_device(0)
@@ -76,6 +79,16 @@ def main():
         ms = timed(lambda: symsyrk_device(Y.data_ptr(), sd.data_ptr(), C.data_ptr(), a.m, k))
         fl = 3 * 2.0 * a.m * k * (k + 1) / 2
         out["rows"] = {"rows": k, "ms": round(ms, 3), "tflops": round(fl / ms / 1e9, 1)}
+    if "gram64" in only:
+        del Y
+        torch.cuda.empty_cache()
+        Y64 = torch.randn(a.n, a.m, device="cuda", generator=g, dtype=torch.float64)
+        sd64 = sd.double()
+        G = torch.empty(a.m, a.m, dtype=torch.float64, device="cuda")
+        ms = timed(lambda: gram_device(Y64.data_ptr(), a.n, a.m, sd64.data_ptr(), G.data_ptr(), FP64))
+        fl = 2.0 * a.n * a.m * (a.m + 1) / 2
+        out["gram64"] = {"ms": round(ms, 3), "tflops": round(fl / ms / 1e9, 2),
+                         "frac_of_nominal_fp64": round(fl / ms / 1e9 / 37.0, 3)}
     print(json.dumps(out))
 
 

@@ -101,8 +101,9 @@ __global__ void __launch_bounds__(256) gemm_tile_kernel(int M, int N, int K, con
 //
 // The m x m Gram of the columns of a row-major n x m matrix (HOOI's dense
 // step in FP64), upper tiles only: 128 x 128 tiles of C, 256 threads with
-// 8 x 8 accumulators each (rows ty*4 + {0..3} and 64 + ty*4 + {0..3}, the
-// same for the columns with tx), k-blocks of 16 rows of A staged in shared
+// 8 x 8 accumulators each (rows 32 q + 2 ty + {0, 1}, q < 4, the same for
+// the columns with tx: a warp's 16-byte loads of one k row are then
+// contiguous and free of bank conflicts), k-blocks of 16 rows of A staged in shared
 // memory by cp.async in a 3-stage ring.  The K axis is cut into splits
 // whose partial tiles the finalize kernel adds (and mirrors).
 constexpr int GB = 128, GK = 16, GST = 3;
@@ -170,16 +171,13 @@ __global__ void __launch_bounds__(256, 1) gram_tn_f64_kernel(int M, int K, const
 #pragma unroll 4
     for (int kk = 0; kk < GK; ++kk) {
       double a[8], b[8];
-      const double2 a0 = *reinterpret_cast<const double2 *>(&As[kk][ty * 4]);
-      const double2 a1 = *reinterpret_cast<const double2 *>(&As[kk][ty * 4 + 2]);
-      const double2 a2 = *reinterpret_cast<const double2 *>(&As[kk][64 + ty * 4]);
-      const double2 a3 = *reinterpret_cast<const double2 *>(&As[kk][64 + ty * 4 + 2]);
-      const double2 b0 = *reinterpret_cast<const double2 *>(&Bs[kk][tx * 4]);
-      const double2 b1 = *reinterpret_cast<const double2 *>(&Bs[kk][tx * 4 + 2]);
-      const double2 b2 = *reinterpret_cast<const double2 *>(&Bs[kk][64 + tx * 4]);
-      const double2 b3 = *reinterpret_cast<const double2 *>(&Bs[kk][64 + tx * 4 + 2]);
-      a[0] = a0.x, a[1] = a0.y, a[2] = a1.x, a[3] = a1.y, a[4] = a2.x, a[5] = a2.y, a[6] = a3.x, a[7] = a3.y;
-      b[0] = b0.x, b[1] = b0.y, b[2] = b1.x, b[3] = b1.y, b[4] = b2.x, b[5] = b2.y, b[6] = b3.x, b[7] = b3.y;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const double2 av = *reinterpret_cast<const double2 *>(&As[kk][32 * q + 2 * ty]);
+        const double2 bv = *reinterpret_cast<const double2 *>(&Bs[kk][32 * q + 2 * tx]);
+        a[2 * q] = av.x, a[2 * q + 1] = av.y;
+        b[2 * q] = bv.x, b[2 * q + 1] = bv.y;
+      }
 #pragma unroll
       for (int i = 0; i < 8; ++i)
 #pragma unroll
@@ -190,11 +188,11 @@ __global__ void __launch_bounds__(256, 1) gram_tn_f64_kernel(int M, int K, const
   double *o = out + blockIdx.y * split_stride;
 #pragma unroll
   for (int i = 0; i < 8; ++i) {
-    const int gi = i0 + (i < 4 ? ty * 4 + i : 64 + ty * 4 + (i - 4));
+    const int gi = i0 + 32 * (i >> 1) + 2 * ty + (i & 1);
     if (gi >= M) continue;
 #pragma unroll
     for (int jh = 0; jh < 4; ++jh) {
-      const int gj = j0 + (jh < 2 ? tx * 4 + 2 * jh : 64 + tx * 4 + 2 * (jh - 2));
+      const int gj = j0 + 32 * jh + 2 * tx;
       if (gj < M) *reinterpret_cast<double2 *>(&o[(size_t)gi * M + gj]) = make_double2(acc[i][2 * jh], acc[i][2 * jh + 1]);
     }
   }
