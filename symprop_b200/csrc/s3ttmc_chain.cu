@@ -47,6 +47,7 @@ constexpr int kSG = 64;   // (s_1, s_2) subgroups per batch
 constexpr int kG = 16;    // s_1 groups per batch
 constexpr int kRP = 16;   // R padded
 constexpr int kM2 = 136;  // packed order-2 entries at R = 16
+constexpr int kS2 = kM2 + 1;  // shared row stride of 16 x kM2 arrays: odd, so rows q, q+1, ... hit different banks
 constexpr int kBeta = 9;  // beta slots per thread: 16 x 9 >= kM2
 
 struct ChainParams {
@@ -86,7 +87,7 @@ template <typename T> struct Smem {
       T Q[kG][kM2];
       T U1[kG][kRP];
     } b;                        // one batch
-    double G[kRP * kM2];        // the row's G at the end (FP64)
+    double G[kRP * kS2];        // the row's G at the end (FP64, row stride kS2)
   } u;
 };
 
@@ -394,13 +395,13 @@ __global__ void __launch_bounds__(kThreads, 4) s3ttmc_chain_kernel(const ChainPa
     __syncthreads();
   }
   // ---- Y = Sym3(G) through shared memory (FP64)
-  double *sG = reinterpret_cast<double *>(&sm.u.b.W[0][0]);  // kRP x kM2
+  double *sG = reinterpret_cast<double *>(&sm.u.b.W[0][0]);  // kRP rows of stride kS2
 #pragma unroll
   for (int a = 0; a < 2; ++a)
 #pragma unroll
     for (int k = 0; k < kBeta; ++k) {
       const int b = b0 + 16 * k;
-      if (b < kM2) sG[(a0 + a) * kM2 + b] = gsum[a][k];
+      if (b < kM2) sG[(a0 + a) * kS2 + b] = gsum[a][k];
     }
   __syncthreads();
   T *Yrow = reinterpret_cast<T *>(p.Y) + (uint64_t)ch.row * p.m3;
@@ -408,8 +409,8 @@ __global__ void __launch_bounds__(kThreads, 4) s3ttmc_chain_kernel(const ChainPa
   for (uint32_t e = tid; e < p.m3; e += kThreads) {
     const uint32_t t3 = p.trip[e];
     const uint32_t q0 = t3 & 0xffu, q1 = (t3 >> 8) & 0xffu, q2 = t3 >> 16;
-    const double y = sG[q0 * kM2 + pair_index(q1, q2, R)] + sG[q1 * kM2 + pair_index(q0, q2, R)] +
-                     sG[q2 * kM2 + pair_index(q0, q1, R)];
+    const double y = sG[q0 * kS2 + pair_index(q1, q2, R)] + sG[q1 * kS2 + pair_index(q0, q2, R)] +
+                     sG[q2 * kS2 + pair_index(q0, q1, R)];
     if (ch.slot == kDirect) Yrow[e] = (T)y;
     else Prow[e] = y;
   }
@@ -433,6 +434,7 @@ __global__ void __launch_bounds__(kThreads, 4) s3ttmc_chain_kernel(const ChainPa
 constexpr int kThreads5 = 256;
 constexpr int kB5 = 128, kH5 = 32, kG5 = 8;
 constexpr int kM3 = 816;                // packed order-3 entries at R = 16
+constexpr int kS3 = kM3 + 1;            // shared row stride of G (odd: conflict-free column reads)
 constexpr int kBeta5 = (kM3 + 63) / 64;  // 13
 
 struct Chain5Params {
@@ -466,9 +468,9 @@ template <typename T> struct Smem5 {
       T U2[kH5][kRP];
       T T2[kG5][kM3];
       T U1[kG5][kRP];
-      T F[2][kRP * kM2];             // F of a group (two buffers)
+      T F[2][kRP * kS2];             // F of a group (two buffers, row stride kS2)
     } b;
-    T G[kRP * kM3];                  // the row's G at the end
+    T G[kRP * kS3];                  // the row's G at the end (row stride kS3)
   } u;
 };
 
@@ -643,7 +645,7 @@ __global__ void __launch_bounds__(kThreads5, (sizeof(T) == 8 ? 1 : 2)) s3ttmc_ch
 #pragma unroll
           for (int j = 0; j < 3; ++j) {
             const int col = c0 + 64 * j;
-            if (col < kM2) F[(r4 + a) * kM2 + col] = f[a][j];
+            if (col < kM2) F[(r4 + a) * kS2 + col] = f[a][j];
           }
         __syncthreads();
         for (int e = tid; e < (int)m3; e += kThreads5) {
@@ -670,13 +672,13 @@ __global__ void __launch_bounds__(kThreads5, (sizeof(T) == 8 ? 1 : 2)) s3ttmc_ch
     __syncthreads();
   }
   // ---- Y = Sym4(G) through shared memory
-  T *sG = sm.u.G;  // kRP x kM3
+  T *sG = sm.u.G;  // kRP rows of stride kS3
 #pragma unroll
   for (int a = 0; a < 4; ++a)
 #pragma unroll
     for (int k = 0; k < kBeta5; ++k) {
       const int b = bg + 64 * k;
-      if (b < kM3) sG[(a4 + a) * kM3 + b] = gsum[a][k];
+      if (b < kM3) sG[(a4 + a) * kS3 + b] = gsum[a][k];
     }
   __syncthreads();
   T *Yrow = reinterpret_cast<T *>(p.Y) + (uint64_t)ch.row * p.m4;
@@ -684,8 +686,8 @@ __global__ void __launch_bounds__(kThreads5, (sizeof(T) == 8 ? 1 : 2)) s3ttmc_ch
   for (uint32_t e = tid; e < p.m4; e += kThreads5) {
     const uint4 qd = p.quad[e];
     const uint32_t q0 = qd.x & 0xffu, q1 = (qd.x >> 8) & 0xffu, q2 = (qd.x >> 16) & 0xffu, q3 = qd.x >> 24;
-    const double y = (double)sG[q0 * kM3 + (qd.y & 0xffffu)] + (double)sG[q1 * kM3 + (qd.y >> 16)] +
-                     (double)sG[q2 * kM3 + (qd.z & 0xffffu)] + (double)sG[q3 * kM3 + (qd.z >> 16)];
+    const double y = (double)sG[q0 * kS3 + (qd.y & 0xffffu)] + (double)sG[q1 * kS3 + (qd.y >> 16)] +
+                     (double)sG[q2 * kS3 + (qd.z & 0xffffu)] + (double)sG[q3 * kS3 + (qd.z >> 16)];
     if (ch.slot == kDirect) Yrow[e] = (T)y;
     else Prow[e] = y;
   }
@@ -985,7 +987,7 @@ const uint32_t *triples(uint32_t R) {
 
 namespace {
 // Order-5 index tables of rank R (kept per device and R): tri[e] for the
-// packed order-3 entry e = (q0 <= q1 <= q2): the offsets in the 16 x kM2
+// packed order-3 entry e = (q0 <= q1 <= q2): the offsets in the 16 x kS2
 // array F of (q0, (q1 q2)), (q1, (q0 q2)) and (q2, (q0 q1)), order-2
 // entries packed; quad[e] for the packed order-4 entry
 // (q0 <= .. <= q3): the q's and the packed order-3 indices of the four
@@ -1012,7 +1014,7 @@ const Order5Tables &order5_tables(uint32_t R) {
   auto Tr = [&](uint32_t a, uint32_t b, uint32_t c) { return (uint32_t)tidx[(a * R + b) * R + c]; };
   std::vector<uint2> tri;
   for_each_sorted(R, 3, [&](const std::vector<uint32_t> &q, uint64_t) {
-    const uint32_t o0 = q[0] * kM2 + P(q[1], q[2]), o1 = q[1] * kM2 + P(q[0], q[2]), o2 = q[2] * kM2 + P(q[0], q[1]);
+    const uint32_t o0 = q[0] * kS2 + P(q[1], q[2]), o1 = q[1] * kS2 + P(q[0], q[2]), o2 = q[2] * kS2 + P(q[0], q[1]);
     tri.push_back(make_uint2(o0 | o1 << 16, o2));
   });
   std::vector<uint4> quad;
