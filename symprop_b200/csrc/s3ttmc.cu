@@ -641,6 +641,10 @@ static void s3ttmc_reserve(TensorState &t, uint32_t R, bool packed, int precisio
   if (slots) t.partials.ensure((size_t)slots * m);
 }
 
+void s3ttmc_prepare(TensorState &t, uint32_t R, bool packed, int precision) {
+  s3ttmc_reserve(t, R, packed, precision);
+}
+
 void s3ttmc_run(TensorState &t, const void *dU, uint32_t R, bool packed, void *dY, int precision,
                 cudaStream_t st) {
   NvtxRange nv("S3TTMc");

@@ -139,6 +139,9 @@ struct TensorState {
 };
 
 // s3ttmc.cu
+// Builds what an S3TTMc of rank R will need (work-item layout, partial-row
+// slots; kept with the tensor), so that a caller can do it ahead of time.
+void s3ttmc_prepare(TensorState &t, uint32_t R, bool packed, int precision);
 void s3ttmc_run(TensorState &t, const void *dU, uint32_t R, bool packed, void *dY,
                 int precision, cudaStream_t stream);
 // host U in, host Y out; the result rows are copied back band by band while

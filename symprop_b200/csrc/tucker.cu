@@ -25,6 +25,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
+#include <future>
 #include <iomanip>
 #include <iostream>
 #include <random>
@@ -147,29 +148,25 @@ int run_tucker(TensorState &t, const symprop_config &c, int alg, symprop_result 
   SPB_CUDA(cudaMemcpy(dD.p, hD.data(), sizeof(double) * m, cudaMemcpyHostToDevice));
   SPB_CUDA(cudaMemcpy(dsD.p, hsD.data(), sizeof(double) * m, cudaMemcpyHostToDevice));
 
-  // factor initialisation
+  // the reference's random factor (std::mt19937(seed), N(0, 1), row-major;
+  // src/tucker.cpp:25-36), drawn on a host thread while the
+  // device buffers are allocated and the S3TTMc layout is built; a user
+  // factor replaces it (and needs no draw)
+  const bool user_init = c.init == SYMPROP_INIT_USER;
+  if (user_init && !res.init_factor) fail(SYMPROP_ERR_INVALID, "init_factor is null");
+  std::vector<double> h0((size_t)n * r);
+  std::future<void> rng;
+  if (user_init) {
+    std::copy(res.init_factor, res.init_factor + h0.size(), h0.begin());
+  } else {
+    rng = std::async(std::launch::async, [&h0, seed = c.seed] {
+      std::normal_distribution<double> distr(0.0, 1.0);
+      std::mt19937 engine{(std::mt19937::result_type)seed};
+      for (double &x : h0) x = distr(engine);
+    });
+  }
   DBuf<double> U((size_t)n * r), Uprev((size_t)n * r);
-  {
-    std::vector<double> h((size_t)n * r);
-    std::normal_distribution<double> distr(0.0, 1.0);
-    std::mt19937 engine{(std::mt19937::result_type)c.seed};
-    for (size_t i = 0; i < h.size(); i++) h[i] = distr(engine);
-    if (c.init == SYMPROP_INIT_USER) {
-      if (!res.init_factor) fail(SYMPROP_ERR_INVALID, "init_factor is null");
-      std::copy(res.init_factor, res.init_factor + h.size(), h.begin());
-    }
-    SPB_CUDA(cudaMemcpy(U.p, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice));
-    // AltHOOI keeps the factor before hosvd_init as factor_prev (spsymtensor.cpp:306-308)
-    SPB_CUDA(cudaMemcpy(Uprev.p, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice));
-  }
-  if (c.init == SYMPROP_INIT_HOSVD) {
-    // non-MKL reference build: prints and leaves the random factor
-    // (src/sparse/matrixops.cpp:15-17)
-    std::printf("Error: sparse SVD requires MKL.\n");
-    std::fflush(stdout);
-  } else if (c.init == SYMPROP_INIT_HOEVD) {
-    hoevd_factor(t, st, r, U.p, c.verbose != 0);
-  }
+  s3ttmc_prepare(t, (uint32_t)r, true, mixed ? SYMPROP_FP32 : SYMPROP_FP64);
 
   const bool gram_nn = n <= m;  // n x n form (AltHOOI's symsyrk) vs m x m Gram
   const int s = gram_nn ? n : m;
@@ -197,6 +194,19 @@ int run_tucker(TensorState &t, const symprop_config &c, int alg, symprop_result 
   DBuf<double> S((size_t)s * s), V((size_t)s * r), Vwarm((size_t)s * r);
   DBuf<double> core((size_t)r * m), core_prev((size_t)r * m), red(2);
   SPB_CUDA(cudaMemsetAsync(core_prev.p, 0, sizeof(double) * r * m, st));
+  // factor initialisation
+  if (rng.valid()) rng.get();
+  SPB_CUDA(cudaMemcpy(U.p, h0.data(), sizeof(double) * h0.size(), cudaMemcpyHostToDevice));
+  // AltHOOI keeps the factor before hosvd_init as factor_prev (spsymtensor.cpp:306-308)
+  SPB_CUDA(cudaMemcpy(Uprev.p, h0.data(), sizeof(double) * h0.size(), cudaMemcpyHostToDevice));
+  if (c.init == SYMPROP_INIT_HOSVD) {
+    // non-MKL reference build: prints and leaves the random factor
+    // (src/sparse/matrixops.cpp:15-17)
+    std::printf("Error: sparse SVD requires MKL.\n");
+    std::fflush(stdout);
+  } else if (c.init == SYMPROP_INIT_HOEVD) {
+    hoevd_factor(t, st, r, U.p, c.verbose != 0);
+  }
   bool have_warm = false;
   std::vector<double> lam(r);
   // Mixed precision: the objective and the convergence test are FP64 (the
