@@ -140,6 +140,7 @@ __global__ void __launch_bounds__(kThreads, 4) s3ttmc_chain_kernel(const ChainPa
   const T *U = reinterpret_cast<const T *>(p.U);
   const T *cc = reinterpret_cast<const T *>(p.c);
   const uint32_t R = p.R, m2 = p.m2;
+  const bool rows16 = R == (uint32_t)kRP && (reinterpret_cast<uintptr_t>(p.U) & 15u) == 0;
 
   for (uint32_t b = tid; b < m2; b += kThreads) {  // lexicographic pairs
     uint32_t x = 0, rem = b;
@@ -200,10 +201,8 @@ __global__ void __launch_bounds__(kThreads, 4) s3ttmc_chain_kernel(const ChainPa
         uint32_t f = rec[h].f;
         if (i == 0) f = 3u;  // a batch starts a group and a subgroup
         fl[h] = (f & 1u) | (((f >> 1) & 1u) << 16);
-        // the W / U2 / U1 stages gather these rows after two barriers
+        // the W stage gathers this row after two barriers
         prefetch_l1(U + (uint64_t)ids.z * R);
-        if (f & 2u) prefetch_l1(U + (uint64_t)ids.y * R);
-        if (f & 1u) prefetch_l1(U + (uint64_t)ids.x * R);
       }
     }
     const uint32_t c1 = cta_scan(fl[0] + fl[1], sm.warp_tot);  // counts through owner 2t+1
@@ -249,6 +248,19 @@ __global__ void __launch_bounds__(kThreads, 4) s3ttmc_chain_kernel(const ChainPa
     // subgroup sizes; the part of a subgroup begun in an earlier lane goes
     // to carry[j] and is added after the barrier, lanes in order.
     {
+      // at R = 16 the s_2 row of every subgroup and the s_1 row of every
+      // group are copied asynchronously while the W gathers run
+      constexpr int kC = kRP * (int)sizeof(T) / 16, kE = 16 / (int)sizeof(T);
+      if (rows16) {
+        for (int e = tid; e < nsg * kC; e += kThreads) {
+          const int sg = e / kC, k = e - sg * kC;
+          cp_async16(&sm.u.b.U2[sg][k * kE], U + (uint64_t)sm.sg_s2[sg] * kRP + k * kE);
+        }
+        for (int e = tid; e < ng * kC; e += kThreads) {
+          const int g = e / kC, k = e - g * kC;
+          cp_async16(&sm.u.b.U1[g][k * kE], U + (uint64_t)sm.g_s1[g] * kRP + k * kE);
+        }
+      }
       constexpr int kLanes = kThreads / 16;
       const int x = tid & 15, j = tid >> 4;
       const int i0 = nb * j / kLanes, i1 = nb * (j + 1) / kLanes;
@@ -285,14 +297,17 @@ __global__ void __launch_bounds__(kThreads, 4) s3ttmc_chain_kernel(const ChainPa
         }
         flush();
       }
-      // the s_2 row of every subgroup and the s_1 row of every group
-      for (int e = tid; e < nsg * kRP; e += kThreads) {
-        const int sg = e >> 4, xx = e & 15;
-        sm.u.b.U2[sg][xx] = (uint32_t)xx < R ? U[(uint64_t)sm.sg_s2[sg] * R + xx] : T(0);
-      }
-      for (int e = tid; e < ng * kRP; e += kThreads) {
-        const int g = e >> 4, xx = e & 15;
-        sm.u.b.U1[g][xx] = (uint32_t)xx < R ? U[(uint64_t)sm.g_s1[g] * R + xx] : T(0);
+      if (rows16) {
+        cp_async_wait_all();
+      } else {  // the s_2 row of every subgroup and the s_1 row of every group
+        for (int e = tid; e < nsg * kRP; e += kThreads) {
+          const int sg = e >> 4, xx = e & 15;
+          sm.u.b.U2[sg][xx] = (uint32_t)xx < R ? U[(uint64_t)sm.sg_s2[sg] * R + xx] : T(0);
+        }
+        for (int e = tid; e < ng * kRP; e += kThreads) {
+          const int g = e >> 4, xx = e & 15;
+          sm.u.b.U1[g][xx] = (uint32_t)xx < R ? U[(uint64_t)sm.g_s1[g] * R + xx] : T(0);
+        }
       }
       __syncthreads();
       if (tid < kRP)
