@@ -24,7 +24,7 @@ struct ChainData {
 // Order 4: rows with at most this many owners share few pivots; the chain
 // schedule hands them to the warp-per-row kernel.  Order 5 keeps every row
 // (the team kernel costs about 9x the chain's FMAs per owner).
-constexpr uint64_t kChainLight = 64;
+constexpr uint64_t kChainLight = 16;
 uint64_t chain_light_max(const TensorState &t);
 
 // Whether the chain schedule covers this tensor and rank.
