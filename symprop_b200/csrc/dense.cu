@@ -198,6 +198,65 @@ __global__ void __launch_bounds__(256, 1) gram_tn_f64_kernel(int M, int K, const
   }
 }
 
+// ------------------------------------ FP64 panel W = A diag(ks) B, N <= 16
+//
+// HOOI's U = Y D^1/2 V and HOQRI's Y D C^T in FP64: a tall row-major A
+// (M x K) times a K x N matrix with N <= 16.  One CTA of 256 threads per 64
+// rows of A, K in blocks of 32 (the A block read once, coalesced along k;
+// the scaled B block broadcast from shared memory); each thread keeps 4
+// outputs (row tid / 4, columns 4 (tid % 4) .. + 3).  HBM-bound on A.
+constexpr int PR = 64, PK = 32;
+
+__global__ void __launch_bounds__(256) panel_f64_kernel(int M, int N, int K, const double *__restrict__ A, int lda,
+                                                        const double *__restrict__ B, int ldb, bool transB,
+                                                        const double *__restrict__ ks, double *__restrict__ W,
+                                                        int ldw) {
+  __shared__ double As[PR][PK + 1];
+  __shared__ __align__(16) double Bs[PK][16];
+  const int tid = threadIdx.x, row = tid >> 2, c0 = (tid & 3) * 4;
+  const int i0 = blockIdx.x * PR;
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int k0 = 0; k0 < K; k0 += PK) {
+    double av[PR * PK / 256];
+#pragma unroll
+    for (int t = 0; t < PR * PK / 256; ++t) {
+      const int e = tid + 256 * t, ii = e / PK, kk = e % PK, gi = i0 + ii, gk = k0 + kk;
+      av[t] = gi < M && gk < K ? A[(size_t)gi * lda + gk] : 0.0;
+    }
+#pragma unroll
+    for (int t = 0; t < PR * PK / 256; ++t) {
+      const int e = tid + 256 * t;
+      As[e / PK][e % PK] = av[t];
+    }
+    for (int e = tid; e < PK * 16; e += 256) {
+      const int kk = e >> 4, q = e & 15, gk = k0 + kk;
+      double b = 0.0;
+      if (gk < K && q < N) {
+        b = transB ? B[(size_t)q * ldb + gk] : B[(size_t)gk * ldb + q];
+        if (ks) b *= ks[gk];
+      }
+      Bs[kk][q] = b;
+    }
+    __syncthreads();
+#pragma unroll 8
+    for (int kk = 0; kk < PK; ++kk) {
+      const double a = As[row][kk];
+      const double2 b0 = *reinterpret_cast<const double2 *>(&Bs[kk][c0]);
+      const double2 b1 = *reinterpret_cast<const double2 *>(&Bs[kk][c0 + 2]);
+      acc[0] = fma(a, b0.x, acc[0]);
+      acc[1] = fma(a, b0.y, acc[1]);
+      acc[2] = fma(a, b1.x, acc[2]);
+      acc[3] = fma(a, b1.y, acc[3]);
+    }
+    __syncthreads();
+  }
+  const int gi = i0 + row;
+  if (gi < M)
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+      if (c0 + j < N) W[(size_t)gi * ldw + c0 + j] = acc[j];
+}
+
 // C = alpha * sum_z P[z] + beta * C, mirroring the lower triangle for sym_upper
 template <typename T>
 __global__ void gemm_finalize_kernel(int M, int N, const T *P, int splits, size_t stride, T alpha,
@@ -638,8 +697,9 @@ struct Scratch {
 // thread per column j, kCoreRB FP64 accumulators, the U rows of the chunk
 // staged in shared memory 64 at a time (every thread reads the same entry).
 constexpr int kCoreRB = 16, kCoreRows = 64;
+template <typename TY>
 __global__ void __launch_bounds__(128) core_partial_kernel(const double *__restrict__ U,
-                                                           const float *__restrict__ Y, int n, int m,
+                                                           const TY *__restrict__ Y, int n, int m,
                                                            int r, int q0, int rows_per_chunk,
                                                            double *__restrict__ P) {
   __shared__ double Us[kCoreRows][kCoreRB];
@@ -731,6 +791,11 @@ void gemm(cudaStream_t st, int M, int N, int K, T alpha, const T *A, int lda, bo
     }
   }
   if constexpr (std::is_same<T, double>::value) {
+    if (!transA && !sym_upper && N <= 16 && M >= 4 * PR && alpha == 1.0 && beta == 0.0) {
+      panel_f64_kernel<<<cdiv(M, PR), 256, 0, st>>>(M, N, K, A, lda, B, ldb, transB, kscale, C, ldc);
+      SPB_LAUNCH_CHECK();
+      return;
+    }
     if (transA && !transB && sym_upper && A == B && lda == ldb && M == N && !kscale && M >= GB && M % 2 == 0 &&
         lda % 2 == 0 && (reinterpret_cast<uintptr_t>(A) & 15) == 0 && alpha == 1.0 && beta == 0.0) {
       gram_f64(st, M, K, A, lda, C, ldc);
@@ -770,7 +835,8 @@ template void gemm<double>(cudaStream_t, int, int, int, double, const double *, 
 template void gemm<float>(cudaStream_t, int, int, int, float, const float *, int, bool,
                           const float *, int, bool, float, float *, int, const float *, bool);
 
-void core_from_f32(cudaStream_t st, const double *U, const float *Y, int n, int m, int r, double *core) {
+template <typename TY>
+static void core_from(cudaStream_t st, const double *U, const TY *Y, int n, int m, int r, double *core) {
   if (r <= 0 || m <= 0) return;
   if (n <= 0) {
     SPB_CUDA(cudaMemsetAsync(core, 0, sizeof(double) * (size_t)r * m, st));
@@ -783,13 +849,20 @@ void core_from_f32(cudaStream_t st, const double *U, const float *Y, int n, int 
   chunks = (int)cdiv(n, rows_per_chunk);
   Scratch part(sizeof(double) * (size_t)chunks * kCoreRB * m, st);
   for (int q0 = 0; q0 < r; q0 += kCoreRB) {
-    core_partial_kernel<<<dim3(colblocks, chunks), 128, 0, st>>>(U, Y, n, m, r, q0, rows_per_chunk,
-                                                                 part.as<double>());
+    core_partial_kernel<TY><<<dim3(colblocks, chunks), 128, 0, st>>>(U, Y, n, m, r, q0, rows_per_chunk,
+                                                                     part.as<double>());
     SPB_LAUNCH_CHECK();
     core_reduce_kernel<<<cdiv((long long)kCoreRB * m, 256), 256, 0, st>>>(part.as<double>(), chunks, m, r, q0,
                                                                           core);
     SPB_LAUNCH_CHECK();
   }
+}
+
+void core_from_f32(cudaStream_t st, const double *U, const float *Y, int n, int m, int r, double *core) {
+  core_from<float>(st, U, Y, n, m, r, core);
+}
+void core_from_f64(cudaStream_t st, const double *U, const double *Y, int n, int m, int r, double *core) {
+  core_from<double>(st, U, Y, n, m, r, core);
 }
 
 template <typename T>

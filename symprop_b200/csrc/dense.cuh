@@ -25,6 +25,8 @@ void gemm(cudaStream_t st, int M, int N, int K, T alpha, const T *A, int lda, bo
 // row-major: Y is read once and widened in registers, FP64 accumulation,
 // deterministic (fixed row chunks summed in order).
 void core_from_f32(cudaStream_t st, const double *U, const float *Y, int n, int m, int r, double *core);
+// the same r x m core U^T Y from an FP64 Y (one read of Y, fixed-order FP64 sums)
+void core_from_f64(cudaStream_t st, const double *U, const double *Y, int n, int m, int r, double *core);
 
 // sum_{i<rows, q<cols} w[q] * (X[i,q] - (Y ? Y[i,q] : 0))^2 and sum w X^2 (FP64 out, deterministic)
 template <typename T>

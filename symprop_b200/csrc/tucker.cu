@@ -300,7 +300,7 @@ int run_tucker(TensorState &t, const symprop_config &c, int alg, symprop_result 
       // the convergence test read it (mixed: from the FP32 Y, widened in
       // registers)
       if (mx) dense::core_from_f32(st, U.p, Y32.p, n, m, r, core.p);
-      else dense::gemm<double>(st, r, m, n, 1.0, U.p, r, true, Y.p, m, false, 0.0, core.p, m);
+      else dense::core_from_f64(st, U.p, Y.p, n, m, r, core.p);
       double h[2];
       if (alg == SYMPROP_HOOI) {
         // rel_residual(core_prev, core) on the unpacked cores
@@ -328,7 +328,7 @@ int run_tucker(TensorState &t, const symprop_config &c, int alg, symprop_result 
         gram::split(st, Y32.p, sD32.p, Z);
         tc_times(core.p, (size_t)m, 1, dsD.p, U.p);
       } else {
-        dense::gemm<double>(st, r, m, n, 1.0, U.p, r, true, Y.p, m, false, 0.0, core.p, m);
+        dense::core_from_f64(st, U.p, Y.p, n, m, r, core.p);
         dense::gemm<double>(st, n, r, m, 1.0, Y.p, m, false, core.p, m, true, 0.0, U.p, r, dD.p);
       }
       dense::orthonormalize(st, U.p, n, r);  // qr (src/dense/matrixops.cpp:58-75)
