@@ -329,6 +329,13 @@ int symprop_ws_predict(const symprop_tensor *t, uint32_t R, uint64_t seed, uint3
 /* ------------------------------------------------------------- devices */
 int symprop_device_count(int *count);
 int symprop_set_device(int device);
+/* The library keeps the scratch of its dense steps (eigensolver blocks,
+ * GEMM and Gram partial sums) in a per-device pool between calls, so that a
+ * repeated solve allocates no new scratch.  This waits for the current
+ * device and returns the pool's unused memory to it (memory in use is not
+ * touched); call it before handing the GPU to other work.  (No reference
+ * counterpart: the reference allocates host memory per call.) */
+int symprop_trim_memory(void);
 
 #ifdef __cplusplus
 }

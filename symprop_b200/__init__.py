@@ -76,6 +76,7 @@ def lib():
         "symprop_last_error": (ctypes.c_char_p, []),
         "symprop_device_count": (_I, [ctypes.POINTER(_I)]),
         "symprop_set_device": (_I, [_I]),
+        "symprop_trim_memory": (_I, []),
         "symprop_tensor_create": (_I, [_U32, _U32, _P, _P, _U64, ctypes.POINTER(_P)]),
         "symprop_tensor_destroy": (_I, [_P]),
         "symprop_tensor_order": (_I, [_P, ctypes.POINTER(_U32)]),
@@ -124,6 +125,7 @@ def lib():
 def exported_symbols() -> list[str]:
     return [
         "symprop_status_string", "symprop_last_error", "symprop_device_count", "symprop_set_device",
+        "symprop_trim_memory",
         "symprop_tensor_create", "symprop_tensor_destroy", "symprop_tensor_order", "symprop_tensor_dim",
         "symprop_tensor_nnz", "symprop_tensor_norm", "symprop_tensor_owner_count", "symprop_tree_build",
         "symprop_tree_level_size", "symprop_tree_owner_count", "symprop_tree_copy_level",
@@ -151,6 +153,12 @@ def device_count() -> int:
     n = _I(0)
     _check(lib().symprop_device_count(ctypes.byref(n)))
     return n.value
+
+
+def trim_memory() -> None:
+    """Return the unused memory of the library's device pool (the dense
+    steps' scratch, kept between calls) to the current device."""
+    _check(lib().symprop_trim_memory())
 
 
 def gram_device(dY_ptr: int, n: int, m: int, dscale_ptr: int, dG_ptr: int, precision: int = FP64,

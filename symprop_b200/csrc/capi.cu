@@ -62,6 +62,13 @@ int symprop_set_device(int device) {
   return guard([&] { SPB_CUDA(cudaSetDevice(device)); });
 }
 
+int symprop_trim_memory(void) {
+  return guard([&] {
+    SPB_CUDA(cudaDeviceSynchronize());
+    SPB_CUDA(cudaMemPoolTrimTo(device_pool(), 0));
+  });
+}
+
 int symprop_tensor_create(uint32_t order, uint32_t dim, const uint32_t *inds, const double *vals,
                           uint64_t nnz, symprop_tensor **out) {
   return guard([&] {

@@ -115,6 +115,9 @@ template <class T> struct DBuf {
   size_t bytes() const { return n * sizeof(T); }
 };
 
+// The library's stream-ordered memory pool of the current device (dense.cu).
+cudaMemPool_t device_pool();
+
 // ------------------------------------------------------- packed indexing
 
 inline uint64_t binom(uint64_t n, uint64_t k) {

@@ -655,30 +655,7 @@ __global__ void residual_kernel(const double *SX, const double *X, int s, int ld
   if (threadIdx.x == 0) res[i] = sqrt(red[0]);
 }
 
-// Stream-ordered scratch from a pool private to this library, one per
-// device, that keeps its memory between calls (release threshold: never):
-// the eigensolver's many small buffers then cost no allocation after the
-// first iteration.  (The device's default pool releases memory at every
-// synchronisation unless its owner raised the threshold.)
-cudaMemPool_t scratch_pool() {
-  static std::mutex mu;
-  static std::map<int, cudaMemPool_t> pools;
-  int dev = 0;
-  SPB_CUDA(cudaGetDevice(&dev));
-  std::lock_guard<std::mutex> lock(mu);
-  auto it = pools.find(dev);
-  if (it != pools.end()) return it->second;
-  cudaMemPoolProps props{};
-  props.allocType = cudaMemAllocationTypePinned;
-  props.location.type = cudaMemLocationTypeDevice;
-  props.location.id = dev;
-  cudaMemPool_t pool;
-  SPB_CUDA(cudaMemPoolCreate(&pool, &props));
-  uint64_t keep = ~0ull;
-  SPB_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
-  pools[dev] = pool;
-  return pool;
-}
+cudaMemPool_t scratch_pool() { return device_pool(); }
 
 struct Scratch {
   void *p = nullptr;
@@ -1093,4 +1070,31 @@ static int top_eigs_op(cudaStream_t st, const SymApply &apply, int s, int r, dou
 }
 
 }  // namespace dense
+
+// Stream-ordered scratch from a pool private to this library, one per
+// device, that keeps its memory between calls (release threshold: never):
+// the eigensolver's many small buffers cost no allocation after the first
+// iteration.  (The device's default pool releases
+// memory at every synchronisation unless its owner raised the threshold.)
+// symprop_trim_memory gives the unused part back.
+cudaMemPool_t device_pool() {
+  static std::mutex mu;
+  static std::map<int, cudaMemPool_t> pools;
+  int dev = 0;
+  SPB_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(mu);
+  auto it = pools.find(dev);
+  if (it != pools.end()) return it->second;
+  cudaMemPoolProps props{};
+  props.allocType = cudaMemAllocationTypePinned;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = dev;
+  cudaMemPool_t pool;
+  SPB_CUDA(cudaMemPoolCreate(&pool, &props));
+  uint64_t keep = ~0ull;
+  SPB_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+  pools[dev] = pool;
+  return pool;
+}
+
 }  // namespace spb

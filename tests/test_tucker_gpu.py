@@ -140,3 +140,23 @@ def test_cli_reads_malformed_text_as_the_reference_loader(gpu, tmp_path):
         return [l.split(" error ")[1] for l in r.stdout.splitlines() if l.startswith("Iteration: ")]
 
     assert errors(bad) == errors(clean)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_repeated_solves_reuse_pool_memory_bit_for_bit(gpu, precision):
+    """The scratch of a solve (eigensolver, GEMM partials, Gram splits) comes
+    from the library's memory pool and stays there after it: a second solve
+    of the same size reuses it, and after symprop_trim_memory a third
+    allocates afresh.  All three give the same error trace and factor bit
+    for bit (n > m: the m x m Gram path)."""
+    t = synth.community_zipf(4, 3000, 60_000, 8, 1.2, 3)
+    X = gpu.SpSymtensor(3000, 4, t, np.ones(t.shape[0]))
+    prec = gpu.PREC_MIXED if precision == "mixed" else gpu.PREC_FP64
+    kw = dict(rank=8, max_iter=6, delta=1.0, seed=0, precision=prec)
+    d1 = X.TuckerHOOI(**kw)
+    d2 = X.TuckerHOOI(**kw)
+    gpu.trim_memory()
+    d3 = X.TuckerHOOI(**kw)
+    for d in (d2, d3):
+        assert np.array_equal(d.error_trace, d1.error_trace)
+        assert np.array_equal(d.factor, d1.factor)
