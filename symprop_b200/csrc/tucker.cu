@@ -129,7 +129,7 @@ int run_tucker(TensorState &t, const symprop_config &c, int alg, symprop_result 
     cudaStream_t s;
     ~StreamGuard() { cudaStreamDestroy(s); }
   } sg{st};
-  Timer tall(st), tphase(st);
+  Timer tall(st), tphase(st), titer(st);
   auto wall0 = std::chrono::steady_clock::now();
   tall.start();
 
@@ -237,6 +237,7 @@ int run_tucker(TensorState &t, const symprop_config &c, int alg, symprop_result 
     std::fprintf(stderr, "tucker: setup %.1f ms (buffers, init)\n",
                  std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - wall0).count());
   for (uint64_t iter = 0; iter < c.max_iter; ++iter) {
+    if (trace) titer.start();
     // eigen-residual target relative to the largest eigenvalue: the FP32 /
     // split-BF16 Gram of the mixed phase resolves about 1e-6 of it
     const double eig_tol = mx ? 1e-5 : fp64_eig_tol;
@@ -349,8 +350,9 @@ int run_tucker(TensorState &t, const symprop_config &c, int alg, symprop_result 
 
     error = std::sqrt(normX * normX - cn2) / normX;
     if (trace) {
-      std::fprintf(stderr, "tucker: iter %llu %s s3ttmc %.1f ms dense %.1f ms error %.12e\n",
-                   (unsigned long long)iter, mx ? "mixed" : "fp64", s3_ms - s3_prev, dense_ms - dense_prev, error);
+      std::fprintf(stderr, "tucker: iter %llu %s s3ttmc %.1f ms dense %.1f ms (iteration %.1f ms) error %.12e\n",
+                   (unsigned long long)iter, mx ? "mixed" : "fp64", s3_ms - s3_prev, dense_ms - dense_prev,
+                   titer.stop_ms(), error);
       s3_prev = s3_ms;
       dense_prev = dense_ms;
     }
@@ -384,6 +386,7 @@ int run_tucker(TensorState &t, const symprop_config &c, int alg, symprop_result 
   }
 
   // outputs
+  const auto wout = std::chrono::steady_clock::now();
   const size_t csize = (size_t)r * full;
   if (res.core) {
     std::vector<double> hc(csize, 0.0);
@@ -404,6 +407,10 @@ int run_tucker(TensorState &t, const symprop_config &c, int alg, symprop_result 
   }
   SPB_CUDA(cudaStreamSynchronize(st));
   res.time_ms = tall.stop_ms();
+  if (trace)
+    std::fprintf(stderr, "tucker: outputs %.1f ms, total %.1f ms\n",
+                 std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - wout).count(),
+                 res.time_ms);
   (void)wall0;
   res.s3ttmc_ms = s3_ms;
   res.dense_ms = dense_ms;
