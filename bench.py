@@ -483,6 +483,7 @@ def main():
 
 HOOI_WORKLOAD = "learned_order5_powerlaw"
 HOOI_RANK, HOOI_TOL, HOOI_DELTA, HOOI_MAX_ITER = 16, 1e-6, 1.0, 100
+HOOI_REPEATS = 3  # runs per arm; the median is reported (host stalls on a shared box move single runs)
 
 
 def _rel_frobenius(A, B, rows_per_chunk=8192):
@@ -559,22 +560,38 @@ def hooi_leg(scale: float = 1.0):
         row.update(extra)
         return Xa, d, row
 
+    def run_median(precision, learned):
+        """HOOI_REPEATS runs of an arm (each from the host tuples: build,
+        prediction, solve); the run of median wall time is reported, with
+        every run's wall time in repeats_ms.  Returns the last run's tensor
+        (all runs build the same one)."""
+        runs = []
+        for k in range(HOOI_REPEATS):
+            Xa, d, row = run_arm(precision, learned)
+            runs.append((row["ms"], d, row))
+            if k + 1 < HOOI_REPEATS:
+                Xa.close()
+        med = sorted(runs, key=lambda x: x[0])[len(runs) // 2]
+        row = dict(med[2], repeats_ms=[r[0] for r in runs])
+        return Xa, med[1], row
+
     out = {"workload": f"{HOOI_WORKLOAD}: order {order}, n={n}, {nnz} tuples, power-law degrees "
                        f"(exponent 2.1), 16 planted communities (80% inside), values 1.0; rank {R} "
                        f"(Y n x {m}); stop at |delta error| < {HOOI_TOL:g}; delta {HOOI_DELTA:g}; seed 0",
            "timing": "wall clock per arm with the device synchronised on both sides, from host tuple "
                      "arrays: tensor build (copy + device build) + prediction (learned arm) + solve; "
+                     f"the median of {HOOI_REPEATS} runs per arm (repeats_ms lists all); "
                      "file I/O and the seeded generator excluded",
            "generator_s": round(gen_s, 1)}
     with ClockSampler(torch.cuda.current_device()) as clk:
-        X64, d64, r64 = run_arm(sp.PREC_FP64, False)
+        X64, d64, r64 = run_median(sp.PREC_FP64, False)
         U64 = d64.factor.copy()
         X64.close()
         del X64
         arms = {"fp64_random": r64}
         for name, prec, learned in (("mixed_learned", sp.PREC_MIXED, True),
                                     ("mixed_random", sp.PREC_MIXED, False)):
-            Xa, d, row = run_arm(prec, learned)
+            Xa, d, row = run_median(prec, learned)
             sv = np.linalg.svd(U64.T @ d.factor, compute_uv=False)
             row["objective_rel_gap_vs_fp64"] = (d.error - d64.error) / d64.error
             row["max_principal_angle_vs_fp64"] = float(np.arccos(np.clip(sv.min(), -1.0, 1.0)))
