@@ -23,7 +23,8 @@ plain copy of Y to the host, the floor the overlapped call approaches.
 (order 5, n = 200,000, 20M power-law tuples, r = 16): plain FP64 HOOI from
 the random start against mixed precision from the learned and the random
 start, each timed to |delta error| < 1e-6 from the host tuple arrays (tensor
-build included, file I/O excluded), with each arm's objective gap, largest
+build included, file I/O excluded; the median of three runs per arm), with
+each arm's objective gap, largest
 principal angle and ||C||^2 error against the FP64 arm, the FP32 S3TTMc's
 relative Frobenius error of Y, and that tensor's FP32 / FP64 S3TTMc rates.
 
