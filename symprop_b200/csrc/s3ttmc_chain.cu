@@ -24,11 +24,13 @@
 // Kernel: one CTA of 128 threads per work item (a row, or a slice of a long
 // row whose partial rows the combine kernel adds).  Owners are taken in
 // batches of up to 256 with at most kSG (s_1, s_2) subgroups and kG s_1
-// groups (43 KB of shared memory in FP64: 4 CTAs per SM); a batch boundary (or slice boundary) may cut a group: by
-// linearity the two parts add up.  Per batch: W of every subgroup, then Q of
-// every group (shared memory), then each thread adds its 18 entries of G.
-// The row's G then goes through shared memory for Sym3.  FP32: the batch's
-// G is summed in FP32 and folded into FP64 totals after every batch.
+// groups (45 KB of shared memory in FP64: 4 CTAs per SM); a batch boundary
+// (or slice boundary) may cut a group: by linearity the two parts add up.
+// Per batch: W of every subgroup (8 lanes over contiguous owner ranges,
+// carries between lanes), then Q of every group as 4 x 4 register tiles
+// (shared memory), then each thread adds its 18 entries of G.  The row's G
+// then goes through shared memory (odd row stride) for Sym3.  FP32: the
+// batch's G is summed in FP32 and folded into FP64 totals after every batch.
 #include <cub/cub.cuh>
 
 #include <algorithm>
@@ -444,8 +446,11 @@ __global__ void __launch_bounds__(kThreads, 4) s3ttmc_chain_kernel(const ChainPa
 // distinct (s_1, s_2) per owner: about 272 + 0.63 * 2448 + 0.19 * 13056
 // FMAs per owner, against about 39,000 for the leaf-by-leaf team kernel.
 // One CTA of 256 threads per work item; batches of up to kB5 owners, kH5
-// (s_1, s_2) prefixes and kG5 s_1 groups.  Each thread keeps 4 x 13 entries
-// of G (rows 4a..4a+3, columns b + 64 k).
+// (s_1, s_2) prefixes and kG5 s_1 groups.  T2 is formed per group as
+// F = sum_h U[s_2] (x) T3_h (16 x m2, register tiles) and one Sym3 of F
+// (T2[q0 q1 q2] = F[q0][q1 q2] + F[q1][q0 q2] + F[q2][q0 q1]), not one Sym3
+// per prefix.  Each thread keeps 4 x 13 entries of G (rows 4a..4a+3,
+// columns b + 64 k).
 constexpr int kThreads5 = 256;
 constexpr int kB5 = 128, kH5 = 32, kG5 = 8;
 constexpr int kM3 = 816;                // packed order-3 entries at R = 16
