@@ -452,7 +452,7 @@ __global__ void __launch_bounds__(kThreads, 4) s3ttmc_chain_kernel(const ChainPa
 // per prefix.  Each thread keeps 4 x 13 entries of G (rows 4a..4a+3,
 // columns b + 64 k).
 constexpr int kThreads5 = 256;
-constexpr int kB5 = 128, kH5 = 32, kG5 = 8;
+constexpr int kB5 = 128, kH5 = 48, kG5 = 12;
 constexpr int kM3 = 816;                // packed order-3 entries at R = 16
 constexpr int kS3 = kM3 + 1;            // shared row stride of G (odd: conflict-free column reads)
 constexpr int kBeta5 = (kM3 + 63) / 64;  // 13
