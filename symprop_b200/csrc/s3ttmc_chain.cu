@@ -45,7 +45,7 @@ namespace {
 
 constexpr int kThreads = 128;
 constexpr int kB = 256;   // owners per batch
-constexpr int kSG = 64;   // (s_1, s_2) subgroups per batch
+constexpr int kSG = 80;   // (s_1, s_2) subgroups per batch
 constexpr int kG = 16;    // s_1 groups per batch
 constexpr int kRP = 16;   // R padded
 constexpr int kM2 = 136;  // packed order-2 entries at R = 16
