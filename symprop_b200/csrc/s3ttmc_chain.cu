@@ -24,7 +24,7 @@
 // Kernel: one CTA of 128 threads per work item (a row, or a slice of a long
 // row whose partial rows the combine kernel adds).  Owners are taken in
 // batches of up to 256 with at most kSG (s_1, s_2) subgroups and kG s_1
-// groups (45 KB of shared memory in FP64: 4 CTAs per SM); a batch boundary
+// groups (49 KB of shared memory in FP64: 4 CTAs per SM); a batch boundary
 // (or slice boundary) may cut a group: by linearity the two parts add up.
 // Per batch: W of every subgroup (8 lanes over contiguous owner ranges,
 // carries between lanes), then Q of every group as 4 x 4 register tiles
